@@ -1,0 +1,358 @@
+"""Benchmark of the B200 CG-SEM elastic time loop.
+
+Workload (N=1): the layered model of 64 x 64 x 32 hexahedra of 250 m,
+polynomial order 4 (5 GLL points per axis, 16.4 M element-local GLL
+points), three flat layers with seeded interface depths and (vp, vs, rho),
+4-element C-PML on x/y/zmax, free surface on top, 2 Hz Ricker point force,
+the x/y/z force directions advanced together in FP32 with FP64
+displacement/velocity accumulation.  One bench "step" is one solver time
+step of all three wavefields over the whole mesh (snapshots of the surface
+recording cells every 10 steps included).
+
+Metric: GLL-point updates per second = n_cell * 125 * n_field * steps / time
+(element-local points, as the reference's "~135M GLL points" count).
+
+Arms:
+  default          this repo's CUDA path through its C ABI (gfb)
+  --impl reference the reference's own CPU functions (oracle/_ref, compiled
+                   from the reference sources; oracle restatement if absent)
+                   on the host cores, one direction per sample step
+
+Multi-GPU (torchrun): independent replicas, one per GPU ("replicas only":
+the directions/models are independent; there is no data-path exchange).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "gf-only-sem_b200")
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # layered model, three directions batched
+    "layered_64x64x32": dict(nx=64, ny=64, nz=32, d=250.0, pml=4, seed=2, src=(8000.0, 8000.0, 2000.0),
+                             nsteps=4000, stride=10, depth=250.0),
+    # configs[0]-shaped halfspace (CPU-runnable size) for quick runs
+    "halfspace_20x20x10": dict(nx=20, ny=20, nz=10, d=500.0, pml=3, seed=0, src=(5000.0, 5000.0, 1000.0),
+                               nsteps=2000, stride=10, depth=500.0),
+}
+
+METRIC = "GLL-point updates/s (FP32 batched x/y/z, 1 B200)"
+UNIT = "GLL-pt/s"
+
+
+def build_workload(name: str):
+    from gfb import mesh
+
+    w = WORKLOADS[name]
+    pml = {"xmin": w["pml"], "xmax": w["pml"], "ymin": w["pml"], "ymax": w["pml"], "zmax": w["pml"]}
+    spec = mesh.MeshSpec(nx=w["nx"], ny=w["ny"], nz=w["nz"], dx=w["d"], dy=w["d"], dz=w["d"], order=4, pml=pml)
+    if name.startswith("layered"):
+        mat = mesh.seeded_layers(w["seed"], w["nz"] * w["d"])
+    else:
+        mat = mesh.homogeneous()
+    return mesh.build_problem(spec, mat, np.array(w["src"]), nsteps=w["nsteps"], snapshot_stride=w["stride"],
+                              record_depth_max_m=w["depth"])
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").strip()
+        ids = [x.strip() for x in vis.split(",") if x.strip()] if vis else []
+        self.device = ids[device] if device < len(ids) else str(device)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def elem_bytes_per_step(prob, info, n_field, prec):
+    """Algorithmic DRAM bytes of one step's element/assembly launches."""
+    nn = 125
+    P = prob["n_cell"] * nn
+    G = prob["n_node"]
+    sr = 4 if prec == 1 else 8
+    F = 3 * n_field
+    geom = P * 12 * sr + P * 4                      # geometry + ibool
+    gather = P * F * sr                              # predicted displacement
+    force = G * F * sr + (P - G) * F * sr * 2        # first touch writes, others read+write
+    Ppml = info["n_pml_cell"] * nn
+    pml = Ppml * (15 * sr + F * 3 * sr * 2 + F * sr * 2 + F * 16 + F * sr)
+    return geom + gather + force + pml
+
+
+def node_bytes_per_step(prob, n_field, prec):
+    sr = 4 if prec == 1 else 8
+    F = 3 * n_field
+    return prob["n_node"] * (F * (32 + 2 * sr + sr + sr) + 8 + (4 if prec == 1 else 0))
+
+
+def committed_traffic():
+    path = os.path.join(REPO, "profiles", "elem_step_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_baseline_sample(prob, seconds_target=20.0):
+    """Reference CPU functions on the host cores: one direction, a few steps
+    of the same mesh (bounded sample)."""
+    import oracle
+
+    which = "ref" if os.path.exists(oracle.LIB_REF) else "oracle"
+    threads = os.cpu_count() or 1
+    run = oracle.Run(prob, 0, which, threads=threads)
+    t0 = time.perf_counter()
+    run.advance(1)
+    t1 = time.perf_counter()
+    step_s = max(t1 - t0, 1e-6)
+    n = max(1, min(20, int(seconds_target / step_s)))
+    t0 = time.perf_counter()
+    run.advance(n)
+    dt = time.perf_counter() - t0
+    run.close()
+    val = prob["n_cell"] * 125 * n / dt
+    return {"value": val, "unit": UNIT, "cores": threads, "kind": "reference" if which == "ref" else "port",
+            "sample": f"{n} FP64 solver steps of direction x on the full mesh after 1 warm-up step "
+                      f"({dt:.1f} s; reference element kernel threaded over cells, rest serial)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+
+    prob = build_workload(args.workload)
+    which = "ref" if os.path.exists(oracle.LIB_REF) else "oracle"
+    threads = os.cpu_count() or 1
+    # one direction stands for each of x/y/z: the three reference runs are
+    # identical in cost (separate processes in the reference, forward.sh)
+    run = oracle.Run(prob, 0, which, threads=threads)
+    run.advance(args.warmup)
+    # bounded: time at most the steps that fit in ~120 s
+    t0 = time.perf_counter()
+    run.advance(1)
+    est = time.perf_counter() - t0
+    n = max(1, min(args.steps, int(120.0 / max(est, 1e-6))))
+    t0 = time.perf_counter()
+    run.advance(n)
+    dt = time.perf_counter() - t0
+    val = prob["n_cell"] * 125 * n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0, "steps": n,
+        "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": dt / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "n_cell": prob["n_cell"], "ngll": 5, "directions": "x (y, z cost the same)"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads,
+                         "kind": "reference" if which == "ref" else "port",
+                         "sample": f"{n} single-direction FP64 solver steps of the full mesh; "
+                                   f"reference functions from oracle/_ref, element kernel threaded over {threads} "
+                                   "threads"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gfb(args):
+    import gfb
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist = tdist
+    device = local if world > 1 else args.device
+    prec = gfb.FP32 if args.precision == "fp32" else gfb.FP64
+    dirs = [0, 1, 2][: args.fields]
+    prob = build_workload(args.workload)
+    s = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8)
+    info = s.info()
+    s.advance(args.warmup)
+    s.drain()
+    s.synchronize()
+
+    def barrier():
+        if dist:
+            import torch
+
+            t = torch.zeros(1, device=f"cuda:{local}")
+            dist.all_reduce(t)
+            torch.cuda.synchronize(local)
+
+    # timed region: K steps; per-phase device time from CUDA events on the
+    # solver's stream; snapshots drained after the region
+    barrier()
+    s.synchronize()
+    launches0 = s.info()["kernel_launches"]
+    with ClockSampler(device) as clk:
+        t0 = time.perf_counter()
+        ms_elem, ms_node, ms_rec = s.advance_profiled(args.steps)
+        s.synchronize()
+        t1 = time.perf_counter()
+    barrier()
+    launches = s.info()["kernel_launches"] - launches0
+    wall = t1 - t0
+    dev_ms = ms_elem + ms_node + ms_rec
+    elapsed = dev_ms / 1e3
+    if dist:
+        import torch
+
+        t = torch.tensor([elapsed], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    units = prob["n_cell"] * 125 * len(dirs) * args.steps * world
+    value = units / elapsed
+    s.drain()
+    s.close()
+
+    # end to end through the public API from host arrays: create (upload and
+    # set-up), K steps, every snapshot read back to host, destroy
+    t0 = time.perf_counter()
+    s2 = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8)
+    up = s2.info()["upload_bytes"]
+    s2.advance(args.steps)
+    rec = s2.drain()
+    s2.synchronize()
+    s2.close()
+    e2e_t = time.perf_counter() - t0
+    rec_bytes = sum(np.asarray(rec[f][k]).size * 8 for f in rec for k in ("strain", "u", "v", "a"))
+    e2e_val = prob["n_cell"] * 125 * len(dirs) * args.steps / e2e_t
+
+    peak, peak_kind = measured_peak_hbm()
+    eb = elem_bytes_per_step(prob, info, len(dirs), prec)
+    achieved = eb / (ms_elem / args.steps / 1e3) / 1e9
+    nb = node_bytes_per_step(prob, len(dirs), prec)
+    traffic = committed_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == gfb.FP32 else "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n_cell": prob["n_cell"], "ngll": 5, "n_node": prob["n_node"],
+                   "fields": len(dirs), "precision": args.precision, "state": "f64 u,v",
+                   "l2": "inputs larger than L2 (geometry alone > 700 MB)", "parallelism": f"replicas{world}",
+                   "n_colour": info["n_colour"], "n_pml_cell": info["n_pml_cell"]},
+        "phases_ms_per_step": {"element": ms_elem / args.steps, "node": ms_node / args.steps,
+                               "record": ms_rec / args.steps, "wall": wall / args.steps * 1e3},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "kernel": "elem_step_kernel (all colour launches of a step)",
+                     "algorithmic_bytes_per_step": eb,
+                     "traffic": (traffic or {}).get("bytes_per_step") if traffic else None},
+        "roofline_node": {"achieved": nb / (ms_node / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                          "algorithmic_bytes_per_step": nb},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": up / args.steps,
+                "d2h_bytes_per_step": rec_bytes / args.steps,
+                "note": "gfb_create from host arrays + K steps + all snapshots read to host + destroy"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(prob)
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gfb", choices=["gfb", "reference"])
+    ap.add_argument("--workload", default="layered_64x64x32", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--fields", type=int, default=3)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gfb(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,988 @@
+// gfb_solver.cu -- host side of the B200 CG-SEM elastic time loop (C ABI in
+// include/gfb.h).  Builds the device layout from the reference's merged
+// partition arrays, launches the kernels of gfb_kernels.cuh and manages the
+// snapshot ring.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/gfb.h"
+#include "gfb_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+gfb_status fail(gfb_status st, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+#define CU(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t _e = (call);                                                           \
+        if (_e != cudaSuccess)                                                             \
+            return fail(_e == cudaErrorMemoryAllocation ? GFB_ERR_NOMEM : GFB_ERR_CUDA,   \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+// GLL nodes, weights and derivative matrix D[i*ng+j] = l_j'(x_i): the
+// tables of forward/share/include/gf/gll.hpp:48-131 (Newton on P_N').
+double legendre(int n, double x) {
+    if (n == 0) return 1.0;
+    if (n == 1) return x;
+    double a = 1.0, b = x, c = 0.0;
+    for (int m = 1; m < n; ++m) {
+        c = ((2.0 * m + 1.0) * x * b - m * a) / (m + 1.0);
+        a = b;
+        b = c;
+    }
+    return c;
+}
+
+double legendre_d(int n, double x) {
+    if (n == 0) return 0.0;
+    if (std::abs(x - 1.0) < 1e-14) return 0.5 * n * (n + 1.0);
+    if (std::abs(x + 1.0) < 1e-14) return (n % 2 == 0 ? -1.0 : 1.0) * 0.5 * n * (n + 1.0);
+    return n * (x * legendre(n, x) - legendre(n - 1, x)) / (x * x - 1.0);
+}
+
+bool gll_tables(int N, std::vector<double>& x, std::vector<double>& w, std::vector<double>& D) {
+    const int ng = N + 1;
+    x.assign(ng, 0.0);
+    w.assign(ng, 0.0);
+    D.assign(ng * ng, 0.0);
+    x[0] = -1.0;
+    x[N] = 1.0;
+    for (int i = 1; i < N; ++i) {
+        double t = -std::cos(M_PI * i / N);
+        for (int it = 0; it < 100; ++it) {
+            const double f = legendre_d(N, t);
+            const double df = (2.0 * t * f - N * (N + 1.0) * legendre(N, t)) / (1.0 - t * t);
+            if (std::abs(df) < 1.0e-14) return false;
+            const double st = -f / df;
+            t += st;
+            if (std::abs(st) < 1.0e-15 * (1.0 + std::abs(t))) break;
+        }
+        x[i] = t;
+    }
+    std::vector<double> pn(ng);
+    for (int i = 0; i < ng; ++i) {
+        pn[i] = legendre(N, x[i]);
+        w[i] = 2.0 / (N * (N + 1.0) * pn[i] * pn[i]);
+    }
+    for (int i = 0; i < ng; ++i)
+        for (int j = 0; j < ng; ++j)
+            D[i * ng + j] = (i == j) ? (i == 0 ? -0.25 * N * (N + 1.0) : (i == N ? 0.25 * N * (N + 1.0) : 0.0))
+                                     : pn[i] / (pn[j] * (x[i] - x[j]));
+    return true;
+}
+
+template <typename F>
+void parallel_for(long long n, F&& fn) {
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n < 65536) nt = 1;
+    if (nt == 1) {
+        fn(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(fn, n * t / nt, n * (t + 1) / nt);
+    for (auto& x : th) x.join();
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+struct Snapshot {
+    int step;
+    int slot;            // device ring slot, or -1 once staged on the host
+    cudaEvent_t done;
+    std::vector<double> host;  // staged copy [NFLD][n_rec][NN][15]
+    int fields_read = 0;
+    std::vector<char> read_mask;
+};
+
+}  // namespace
+
+struct gfb_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;
+    int prec = GFB_FP64;
+    int ng = 0, nn = 0, nfld = 1, F = 3;
+    int n_cell = 0, n_node = 0;
+    double dt = 0.0;
+    int stride = 0;
+    int dirs[3] = {0, 1, 2};
+    int step = 0;
+    std::vector<int> colour_begin;  // [n_colour+1] device cell ranges
+    std::vector<double> stf;
+    bool has_cpml = false, has_damping = false, has_src = false;
+    int n_pml = 0, n_src = 0, n_rec = 0, slots = 0;
+    double c1 = 0.0, c2 = 0.0;
+    // device memory
+    std::vector<std::unique_ptr<DevBuf>> bufs;
+    uint32_t* ibool = nullptr;
+    void* geom = nullptr;
+    void* dmat = nullptr;
+    double *u = nullptr, *v = nullptr;
+    void *a = nullptr, *ut = nullptr, *force = nullptr;
+    double* mass = nullptr;
+    void* inv_mass = nullptr;
+    double* damping = nullptr;
+    int* pml_slot = nullptr;
+    void *pml_coef = nullptr, *pml_mem = nullptr, *pml_prev = nullptr;
+    int *src_head = nullptr, *src_next = nullptr;
+    void* src_w = nullptr;
+    int* rec_cell = nullptr;
+    double* ring = nullptr;
+    std::deque<Snapshot> pending;
+    std::vector<int> free_slots;
+    long long device_bytes = 0, upload_bytes = 0, launches = 0;
+
+    template <typename T>
+    gfb_status alloc(T** out, size_t count) {
+        auto b = std::make_unique<DevBuf>();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&b->p, count * sizeof(T));
+        if (e != cudaSuccess)
+            return fail(GFB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
+                        cudaGetErrorString(e));
+        *out = static_cast<T*>(b->p);
+        device_bytes += (long long)(count * sizeof(T));
+        bufs.push_back(std::move(b));
+        return GFB_OK;
+    }
+    ~gfb_solver() {
+        for (auto& s : pending)
+            if (s.done) cudaEventDestroy(s.done);
+        bufs.clear();
+        if (stream) cudaStreamDestroy(stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+    }
+};
+
+namespace {
+
+template <typename Real>
+gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
+    Real* d = nullptr;
+    gfb_status st = s->alloc(&d, h.size());
+    if (st) return st;
+    CU(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(Real), cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->upload_bytes += (long long)(h.size() * sizeof(Real));
+    *dst = d;
+    return GFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel dispatch
+// ---------------------------------------------------------------------------
+
+template <typename Real, int NG, int NFLD>
+gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
+    using S = gfb::Shape<NG>;
+    gfb::ElemArgs<Real> A;
+    A.e_begin = s->colour_begin[c];
+    A.e_end = s->colour_begin[c + 1];
+    if (A.e_end <= A.e_begin) return GFB_OK;
+    A.ibool = s->ibool;
+    A.geom = static_cast<const Real*>(s->geom);
+    A.ut = static_cast<const Real*>(s->ut);
+    A.force = static_cast<Real*>(s->force);
+    A.dmat = static_cast<const Real*>(s->dmat);
+    A.pml_slot = s->has_cpml ? s->pml_slot : nullptr;
+    A.pml_coef = static_cast<const Real*>(s->pml_coef);
+    A.pml_mem = static_cast<Real*>(s->pml_mem);
+    A.pml_prev = static_cast<Real*>(s->pml_prev);
+    A.u = s->u;
+    A.v = s->v;
+    A.a = static_cast<const Real*>(s->a);
+    A.c1 = s->c1;
+    A.c2 = s->c2;
+    A.src_head = s->has_src ? s->src_head : nullptr;
+    A.src_next = s->src_next;
+    A.src_w = static_cast<const Real*>(s->src_w);
+    A.stf = stf;
+    A.dir0 = s->dirs[0];
+    A.dir1 = s->dirs[1];
+    A.dir2 = s->dirs[2];
+    const int n = A.e_end - A.e_begin;
+    const int blocks = (n + S::EPB - 1) / S::EPB;
+    const size_t smem = gfb::elem_smem_bytes<Real, NG, NFLD>();
+    gfb::elem_step_kernel<Real, NG, NFLD><<<blocks, S::THREADS, smem, s->stream>>>(A);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+template <typename Real, int NG, int NFLD>
+gfb_status set_smem_t() {
+    const size_t smem = gfb::elem_smem_bytes<Real, NG, NFLD>();
+    CU(cudaFuncSetAttribute(gfb::elem_step_kernel<Real, NG, NFLD>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return GFB_OK;
+}
+
+template <typename Real, int NG, int NFLD>
+gfb_status launch_record_t(gfb_solver* s, double* out) {
+    using S = gfb::Shape<NG>;
+    gfb::RecArgs<Real> A;
+    A.n_rec = s->n_rec;
+    A.rec_cell = s->rec_cell;
+    A.ibool = s->ibool;
+    A.geom = static_cast<const Real*>(s->geom);
+    A.dmat = static_cast<const Real*>(s->dmat);
+    A.u = s->u;
+    A.v = s->v;
+    A.a = static_cast<const Real*>(s->a);
+    A.out = out;
+    gfb::record_kernel<Real, NG, NFLD><<<s->n_rec, S::NNP, 0, s->stream>>>(A);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+// Instantiate (Real, NG, NFLD) combinations behind one switch.
+template <typename Real, template <typename, int, int> class Op, typename... Args>
+gfb_status dispatch(int ng, int nfld, Args... args) {
+#define GFB_CASE(NGV, NFV) \
+    if (ng == NGV && nfld == NFV) return Op<Real, NGV, NFV>::run(args...);
+    GFB_CASE(3, 1) GFB_CASE(3, 2) GFB_CASE(3, 3)
+    GFB_CASE(4, 1) GFB_CASE(4, 2) GFB_CASE(4, 3)
+    GFB_CASE(5, 1) GFB_CASE(5, 2) GFB_CASE(5, 3)
+    GFB_CASE(6, 1) GFB_CASE(6, 2) GFB_CASE(6, 3)
+#undef GFB_CASE
+    return fail(GFB_ERR_UNSUPPORTED, "ngll=%d with %d wavefields is not supported", ng, nfld);
+}
+
+template <typename Real, int NG, int NFLD>
+struct ElemOp {
+    static gfb_status run(gfb_solver* s, int c, double stf) { return launch_elem_t<Real, NG, NFLD>(s, c, (Real)stf); }
+};
+template <typename Real, int NG, int NFLD>
+struct SmemOp {
+    static gfb_status run() { return set_smem_t<Real, NG, NFLD>(); }
+};
+template <typename Real, int NG, int NFLD>
+struct RecOp {
+    static gfb_status run(gfb_solver* s, double* out) { return launch_record_t<Real, NG, NFLD>(s, out); }
+};
+
+gfb_status launch_elem(gfb_solver* s, int c, double stf) {
+    if (s->prec == GFB_FP64) return dispatch<double, ElemOp>(s->ng, s->nfld, s, c, stf);
+    return dispatch<float, ElemOp>(s->ng, s->nfld, s, c, stf);
+}
+
+gfb_status launch_record(gfb_solver* s, double* out) {
+    if (s->prec == GFB_FP64) return dispatch<double, RecOp>(s->ng, s->nfld, s, out);
+    return dispatch<float, RecOp>(s->ng, s->nfld, s, out);
+}
+
+int grid_for(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    return (int)std::max(1LL, std::min(b, 148LL * 32));
+}
+
+template <typename Real>
+gfb_status launch_node_t(gfb_solver* s) {
+    gfb::NodeArgs<Real> A;
+    A.n = (long long)s->n_node * s->F;
+    A.F = s->F;
+    A.u = s->u;
+    A.v = s->v;
+    A.a = static_cast<Real*>(s->a);
+    A.ut = static_cast<Real*>(s->ut);
+    A.force = static_cast<const Real*>(s->force);
+    A.mass = s->mass;
+    A.inv_mass = static_cast<const Real*>(s->inv_mass);
+    A.damping = s->has_damping ? s->damping : nullptr;
+    A.dt = s->dt;
+    A.beta = 0.0;
+    A.gamma = 0.5;
+    A.half_dt2 = 0.5 * s->dt * s->dt * (1.0 - 2.0 * A.beta);
+    gfb::node_update_kernel<Real><<<grid_for(A.n, 256), 256, 0, s->stream>>>(A);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+gfb_status launch_node(gfb_solver* s) {
+    return s->prec == GFB_FP64 ? launch_node_t<double>(s) : launch_node_t<float>(s);
+}
+
+template <typename Real>
+gfb_status launch_predict_t(gfb_solver* s) {
+    const long long n = (long long)s->n_node * s->F;
+    const double h = 0.5 * s->dt * s->dt * (1.0 - 2.0 * 0.0);
+    gfb::predict_kernel<Real><<<grid_for(n, 256), 256, 0, s->stream>>>(
+        n, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+gfb_status launch_predict(gfb_solver* s) {
+    return s->prec == GFB_FP64 ? launch_predict_t<double>(s) : launch_predict_t<float>(s);
+}
+
+size_t snapshot_doubles(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
+
+// Move the oldest device-resident snapshot to host memory, freeing its slot.
+gfb_status stage_oldest(gfb_solver* s) {
+    for (auto& snap : s->pending) {
+        if (snap.slot < 0) continue;
+        CU(cudaEventSynchronize(snap.done));
+        snap.host.resize(snapshot_doubles(s));
+        CU(cudaMemcpy(snap.host.data(), s->ring + (size_t)snap.slot * snapshot_doubles(s),
+                      snap.host.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        s->free_slots.push_back(snap.slot);
+        snap.slot = -1;
+        return GFB_OK;
+    }
+    return fail(GFB_ERR_STATE, "no device snapshot to stage");
+}
+
+// ---------------------------------------------------------------------------
+// solver construction
+// ---------------------------------------------------------------------------
+
+template <typename Real>
+gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
+                        const std::vector<int>& perm, const std::vector<int>& inv_perm,
+                        const std::vector<uint32_t>& ibool_dev, const std::vector<double>& node_mass,
+                        const std::vector<double>& node_damp, const std::vector<double>& w,
+                        const std::vector<double>& D) {
+    const int ng = s->ng, nn = s->nn;
+    const long long n_cell = s->n_cell;
+    gfb_status st;
+    // ibool
+    {
+        uint32_t* d = nullptr;
+        if ((st = s->alloc(&d, ibool_dev.size()))) return st;
+        CU(cudaMemcpy(d, ibool_dev.data(), ibool_dev.size() * 4, cudaMemcpyHostToDevice));
+        s->upload_bytes += (long long)ibool_dev.size() * 4;
+        s->ibool = d;
+    }
+    // geometry [cell][12][NN] in colour order
+    {
+        std::vector<Real> g((size_t)n_cell * 12 * nn);
+        parallel_for(n_cell, [&](long long e0, long long e1) {
+            for (long long ed = e0; ed < e1; ++ed) {
+                const long long e = perm[ed];
+                Real* o = g.data() + ed * 12 * nn;
+                for (int p = 0; p < nn; ++p) {
+                    const long long q = e * nn + p;
+                    for (int f = 0; f < 9; ++f) o[f * nn + p] = (Real)m->dxi_dx[q * 9 + f];
+                    const int i = p / (ng * ng), j = (p / ng) % ng, k = p % ng;
+                    // factor = detJ * w_i * w_j * w_k (element_cpu.cpp:108)
+                    o[9 * nn + p] = (Real)(m->jacobian[q] * w[i] * w[j] * w[k]);
+                    o[10 * nn + p] = (Real)m->lambda_[q];
+                    o[11 * nn + p] = (Real)m->mu[q];
+                }
+            }
+        });
+        if ((st = upload(s, &s->geom, g))) return st;
+    }
+    {
+        std::vector<Real> d(D.size());
+        for (size_t i = 0; i < D.size(); ++i) d[i] = (Real)D[i];
+        if ((st = upload(s, &s->dmat, d))) return st;
+    }
+    const long long nF = (long long)s->n_node * s->F;
+    if ((st = s->alloc(&s->u, nF))) return st;
+    if ((st = s->alloc(&s->v, nF))) return st;
+    Real* a = nullptr;
+    Real* ut = nullptr;
+    Real* force = nullptr;
+    if ((st = s->alloc(&a, nF))) return st;
+    if ((st = s->alloc(&ut, nF))) return st;
+    if ((st = s->alloc(&force, nF))) return st;
+    s->a = a;
+    s->ut = ut;
+    s->force = force;
+    CU(cudaMemset(s->u, 0, nF * sizeof(double)));
+    CU(cudaMemset(s->v, 0, nF * sizeof(double)));
+    CU(cudaMemset(a, 0, nF * sizeof(Real)));
+    CU(cudaMemset(ut, 0, nF * sizeof(Real)));
+    CU(cudaMemset(force, 0, nF * sizeof(Real)));
+    {
+        double* d = nullptr;
+        if ((st = s->alloc(&d, node_mass.size()))) return st;
+        CU(cudaMemcpy(d, node_mass.data(), node_mass.size() * 8, cudaMemcpyHostToDevice));
+        s->upload_bytes += (long long)node_mass.size() * 8;
+        s->mass = d;
+    }
+    if (s->prec == GFB_FP32) {
+        std::vector<Real> im(node_mass.size());
+        for (size_t g = 0; g < im.size(); ++g) im[g] = node_mass[g] > 0.0 ? (Real)(1.0 / node_mass[g]) : Real(0);
+        if ((st = upload(s, &s->inv_mass, im))) return st;
+    }
+    if (s->has_damping) {
+        double* d = nullptr;
+        if ((st = s->alloc(&d, node_damp.size()))) return st;
+        CU(cudaMemcpy(d, node_damp.data(), node_damp.size() * 8, cudaMemcpyHostToDevice));
+        s->damping = d;
+    }
+    // C-PML cells
+    if (s->has_cpml) {
+        std::vector<int> slot(n_cell, -1);
+        std::vector<long long> slot_cell;
+        for (long long ed = 0; ed < n_cell; ++ed)
+            if (m->pml_region[perm[ed]] != 0) {
+                slot[ed] = (int)slot_cell.size();
+                slot_cell.push_back(perm[ed]);
+            }
+        s->n_pml = (int)slot_cell.size();
+        {
+            int* d = nullptr;
+            if ((st = s->alloc(&d, slot.size()))) return st;
+            CU(cudaMemcpy(d, slot.data(), slot.size() * 4, cudaMemcpyHostToDevice));
+            s->pml_slot = d;
+        }
+        std::vector<Real> coef((size_t)s->n_pml * 15 * nn);
+        parallel_for(s->n_pml, [&](long long a0, long long a1) {
+            for (long long sl = a0; sl < a1; ++sl) {
+                const long long e = slot_cell[sl];
+                Real* o = coef.data() + sl * 15 * nn;
+                for (int p = 0; p < nn; ++p) {
+                    const long long q = e * nn + p;
+                    for (int f = 0; f < 9; ++f) o[f * nn + p] = (Real)m->pml_coef_alpha[q * 9 + f];
+                    for (int f = 0; f < 5; ++f) o[(9 + f) * nn + p] = (Real)m->pml_coef_abar[q * 5 + f];
+                    const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
+                    const double wgll = w[ni] * w[nj] * w[nk];  // pml.cpp:171-174
+                    const double rho = m->density[q];
+                    const double rho_inv = (rho > 0.0) ? 1.0 / rho : 0.0;
+                    o[14 * nn + p] = (Real)(wgll * rho_inv * m->jacobian[q]);
+                }
+            }
+        });
+        if ((st = upload(s, &s->pml_coef, coef))) return st;
+        Real *mem = nullptr, *prev = nullptr;
+        if ((st = s->alloc(&mem, (size_t)s->n_pml * s->F * 3 * nn))) return st;
+        if ((st = s->alloc(&prev, (size_t)s->n_pml * s->F * nn))) return st;
+        CU(cudaMemset(mem, 0, (size_t)s->n_pml * s->F * 3 * nn * sizeof(Real)));
+        CU(cudaMemset(prev, 0, (size_t)s->n_pml * s->F * nn * sizeof(Real)));
+        s->pml_mem = mem;
+        s->pml_prev = prev;
+    }
+    // source: cells located by id (solver.cpp:250-258), chained per cell
+    if (src && src->n_src_cell > 0) {
+        std::vector<int> head(n_cell, -1), next(src->n_src_cell, -1), tail(n_cell, -1);
+        std::vector<Real> wts((size_t)src->n_src_cell * nn, Real(0));
+        int used = 0;
+        for (int si = 0; si < src->n_src_cell; ++si) {
+            long long found = -1;
+            for (long long e = 0; e < n_cell; ++e) {
+                const long long id = m->cell_ids ? m->cell_ids[e] : e;
+                if (id == src->cell_ids[si]) {
+                    found = e;
+                    break;
+                }
+            }
+            if (found < 0) continue;  // not in this mesh (reference: -1, skipped)
+            const int ed = inv_perm[found];
+            for (int p = 0; p < nn; ++p) wts[(size_t)si * nn + p] = (Real)src->weights[(size_t)si * nn + p];
+            if (head[ed] < 0) head[ed] = si;
+            else next[tail[ed]] = si;
+            tail[ed] = si;
+            ++used;
+        }
+        s->has_src = used > 0;
+        s->n_src = src->n_src_cell;
+        int *dh = nullptr, *dn = nullptr;
+        if ((st = s->alloc(&dh, head.size()))) return st;
+        if ((st = s->alloc(&dn, next.size()))) return st;
+        CU(cudaMemcpy(dh, head.data(), head.size() * 4, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dn, next.data(), next.size() * 4, cudaMemcpyHostToDevice));
+        s->src_head = dh;
+        s->src_next = dn;
+        if ((st = upload(s, &s->src_w, wts))) return st;
+        s->stf.assign(src->stf, src->stf + std::max(0, src->n_stf));
+    }
+    // recording cells and snapshot ring
+    if (s->n_rec > 0) {
+        std::vector<int> rc(s->n_rec);
+        for (int ci = 0; ci < s->n_rec; ++ci) rc[ci] = inv_perm[m->rec_cell_local[ci]];
+        int* d = nullptr;
+        if ((st = s->alloc(&d, rc.size()))) return st;
+        CU(cudaMemcpy(d, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice));
+        s->rec_cell = d;
+        if ((st = s->alloc(&s->ring, snapshot_doubles(s) * s->slots))) return st;
+        for (int k = s->slots - 1; k >= 0; --k) s->free_slots.push_back(k);
+    }
+    return GFB_OK;
+}
+
+gfb_status validate(const gfb_mesh* m, const gfb_config* c) {
+    if (!m || !c) return fail(GFB_ERR_INVALID, "mesh and config are required");
+    if (m->ngll < 3 || m->ngll > 6)
+        return fail(GFB_ERR_UNSUPPORTED, "ngll=%d outside the supported 3..6", m->ngll);
+    if (m->n_cell <= 0) return fail(GFB_ERR_INVALID, "n_cell must be positive (got %d)", m->n_cell);
+    if (m->n_node <= 0 || (uint32_t)m->n_node > gfb::kNodeMask)
+        return fail(GFB_ERR_INVALID, "n_node=%d out of range", m->n_node);
+    if (!m->ibool || !m->dxi_dx || !m->jacobian || !m->lambda_ || !m->mu || !m->mass)
+        return fail(GFB_ERR_INVALID, "ibool, dxi_dx, jacobian, lambda, mu and mass are required");
+    if (m->pml_coef_abar && (!m->pml_region || !m->pml_coef_alpha || !m->density))
+        return fail(GFB_ERR_INVALID, "C-PML needs pml_region, pml_coef_alpha and density");
+    if (!(c->dt > 0.0)) return fail(GFB_ERR_INVALID, "dt must be positive");
+    if (c->precision != GFB_FP64 && c->precision != GFB_FP32)
+        return fail(GFB_ERR_INVALID, "unknown precision %d", c->precision);
+    if (c->n_field < 1 || c->n_field > 3) return fail(GFB_ERR_INVALID, "n_field must be 1..3");
+    for (int d = 0; d < c->n_field; ++d)
+        if (c->field_dir[d] < 0 || c->field_dir[d] > 2)
+            return fail(GFB_ERR_INVALID, "field_dir[%d]=%d must be 0, 1 or 2", d, c->field_dir[d]);
+    if (m->n_rec_cell < 0 || (m->n_rec_cell > 0 && !m->rec_cell_local))
+        return fail(GFB_ERR_INVALID, "bad recording map");
+    for (int ci = 0; ci < m->n_rec_cell; ++ci)
+        if (m->rec_cell_local[ci] < 0 || m->rec_cell_local[ci] >= m->n_cell)
+            return fail(GFB_ERR_INVALID, "rec_cell_local[%d]=%d out of range", ci, m->rec_cell_local[ci]);
+    return GFB_OK;
+}
+
+
+// One solver step: NC colour launches, node update, optional snapshot.
+// With ev != nullptr, events 0..3 bracket the three phases on the stream.
+gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
+    gfb_status st;
+    const int n_colour = (int)s->colour_begin.size() - 1;
+    const int step = s->step;
+    const double stf = (s->has_src && step < (int)s->stf.size()) ? s->stf[step] : 0.0;
+    if (ev) CU(cudaEventRecord(ev[0], s->stream));
+    for (int c = 0; c < n_colour; ++c)
+        if ((st = launch_elem(s, c, stf))) return st;
+    if (ev) CU(cudaEventRecord(ev[1], s->stream));
+    if ((st = launch_node(s))) return st;
+    if (ev) CU(cudaEventRecord(ev[2], s->stream));
+    if (s->stride > 0 && s->n_rec > 0 && step % s->stride == 0) {
+        if (s->free_slots.empty())
+            if ((st = stage_oldest(s))) return st;
+        const int slot = s->free_slots.back();
+        s->free_slots.pop_back();
+        if ((st = launch_record(s, s->ring + (size_t)slot * snapshot_doubles(s)))) return st;
+        Snapshot snap;
+        snap.step = step;
+        snap.slot = slot;
+        CU(cudaEventCreateWithFlags(&snap.done, cudaEventDisableTiming));
+        CU(cudaEventRecord(snap.done, s->stream));
+        snap.read_mask.assign(s->nfld, 0);
+        s->pending.push_back(std::move(snap));
+    }
+    if (ev) CU(cudaEventRecord(ev[3], s->stream));
+    s->step++;
+    return GFB_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+int32_t gfb_abi_version(void) { return GFB_ABI_VERSION; }
+
+const char* gfb_last_error(void) { return g_err.c_str(); }
+
+gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, gfb_solver** out) {
+    if (!out) return fail(GFB_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    gfb_status st = validate(m, c);
+    if (st) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(GFB_ERR_NO_DEVICE, "no CUDA-capable GPU found");
+    if (c->device < 0 || c->device >= ndev) return fail(GFB_ERR_INVALID, "device %d not present", c->device);
+    CU(cudaSetDevice(c->device));
+
+    auto s = std::make_unique<gfb_solver>();
+    s->device = c->device;
+    s->prec = c->precision;
+    s->ng = m->ngll;
+    s->nn = m->ngll * m->ngll * m->ngll;
+    s->nfld = c->n_field;
+    s->F = 3 * c->n_field;
+    s->n_cell = m->n_cell;
+    s->n_node = m->n_node;
+    s->dt = c->dt;
+    s->stride = c->snapshot_stride;
+    for (int d = 0; d < 3; ++d) s->dirs[d] = d < c->n_field ? c->field_dir[d] : 0;
+    s->has_cpml = m->pml_coef_abar != nullptr;
+    s->n_rec = m->n_rec_cell;
+    s->slots = std::max(1, c->record_slots);
+    const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
+    s->c1 = (1.0 - 2.0 * theta) * 0.5 * c->dt;
+    s->c2 = (1.0 - theta) * 0.5 * c->dt * c->dt;
+    CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+
+    const int nn = s->nn;
+    const long long P = (long long)m->n_cell * nn;
+    // ibool range and per-cell distinctness (a repeated node inside one cell
+    // would make two threads of one block update the same force entry)
+    std::vector<int> mark(m->n_node, -1);
+    for (long long e = 0; e < m->n_cell; ++e)
+        for (int p = 0; p < nn; ++p) {
+            const int g = m->ibool[e * nn + p];
+            if (g < 0 || g >= m->n_node)
+                return fail(GFB_ERR_INVALID, "ibool[%lld]=%d outside [0,%d)", e * nn + p, g, m->n_node);
+            if (mark[g] == (int)e)
+                return fail(GFB_ERR_INVALID, "cell %lld lists node %d twice", e, g);
+            mark[g] = (int)e;
+        }
+    // global lumped mass (accumulate) and damping (assign), solver.cpp:193-202
+    std::vector<double> node_mass(m->n_node, 0.0), node_damp(m->n_node, 0.0);
+    for (long long q = 0; q < P; ++q) {
+        const int g = m->ibool[q];
+        node_mass[g] += m->mass[q];
+        node_damp[g] = m->damping ? m->damping[q] : 0.0;
+    }
+    s->has_damping = false;
+    if (!s->has_cpml && m->damping)
+        for (double d : node_damp)
+            if (d > 0.0) {
+                s->has_damping = true;
+                break;
+            }
+    // greedy colouring in cell order: colour = lowest colour unused by any
+    // cell already sharing a node (structured meshes get the 8 parity colours)
+    std::vector<uint64_t> used(m->n_node, 0);
+    std::vector<int> colour(m->n_cell);
+    int n_colour = 0;
+    for (long long e = 0; e < m->n_cell; ++e) {
+        uint64_t u = 0;
+        for (int p = 0; p < nn; ++p) u |= used[m->ibool[e * nn + p]];
+        if (~u == 0) return fail(GFB_ERR_UNSUPPORTED, "mesh needs more than 64 colours");
+        const int col = __builtin_ctzll(~u);
+        colour[e] = col;
+        n_colour = std::max(n_colour, col + 1);
+        for (int p = 0; p < nn; ++p) used[m->ibool[e * nn + p]] |= (1ull << col);
+    }
+    std::vector<int> perm(m->n_cell), inv_perm(m->n_cell);
+    s->colour_begin.assign(n_colour + 1, 0);
+    for (long long e = 0; e < m->n_cell; ++e) s->colour_begin[colour[e] + 1]++;
+    for (int k = 0; k < n_colour; ++k) s->colour_begin[k + 1] += s->colour_begin[k];
+    {
+        std::vector<int> fill(s->colour_begin.begin(), s->colour_begin.end() - 1);
+        for (long long e = 0; e < m->n_cell; ++e) {
+            const int ed = fill[colour[e]]++;
+            perm[ed] = (int)e;
+            inv_perm[e] = ed;
+        }
+    }
+    // device ibool with the first-touch bit: the lowest colour touching a
+    // node stores, later colours add
+    std::vector<uint32_t> ibool_dev((size_t)P);
+    parallel_for(m->n_cell, [&](long long e0, long long e1) {
+        for (long long ed = e0; ed < e1; ++ed) {
+            const long long e = perm[ed];
+            for (int p = 0; p < nn; ++p) {
+                const uint32_t g = (uint32_t)m->ibool[e * nn + p];
+                const bool first = __builtin_ctzll(used[g]) == colour[e];
+                ibool_dev[ed * nn + p] = g | (first ? gfb::kFirstTouch : 0u);
+            }
+        }
+    });
+    std::vector<double> x, w, D;
+    if (!gll_tables(m->ngll - 1, x, w, D)) return fail(GFB_ERR_INVALID, "GLL table construction failed");
+    if (s->prec == GFB_FP64) {
+        if ((st = dispatch<double, SmemOp>(s->ng, s->nfld))) return st;
+        st = build_device<double>(s.get(), m, src, perm, inv_perm, ibool_dev, node_mass, node_damp, w, D);
+    } else {
+        if ((st = dispatch<float, SmemOp>(s->ng, s->nfld))) return st;
+        st = build_device<float>(s.get(), m, src, perm, inv_perm, ibool_dev, node_mass, node_damp, w, D);
+    }
+    if (st) return st;
+    CU(cudaStreamSynchronize(s->stream));
+    CU(cudaDeviceSynchronize());
+    *out = s.release();
+    return GFB_OK;
+}
+
+gfb_status gfb_destroy(gfb_solver* s) {
+    if (!s) return GFB_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+    return GFB_OK;
+}
+
+gfb_status gfb_advance(gfb_solver* s, int32_t n_steps) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (n_steps < 0) return fail(GFB_ERR_INVALID, "n_steps must be >= 0");
+    CU(cudaSetDevice(s->device));
+    for (int it = 0; it < n_steps; ++it) {
+        gfb_status st = one_step(s, nullptr);
+        if (st) return st;
+    }
+    return GFB_OK;
+}
+
+gfb_status gfb_advance_profiled(gfb_solver* s, int32_t n_steps, double* ms_element, double* ms_node,
+                                double* ms_record) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (n_steps < 0) return fail(GFB_ERR_INVALID, "n_steps must be >= 0");
+    CU(cudaSetDevice(s->device));
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CU(cudaEventCreate(&e));
+    double acc[3] = {0, 0, 0};
+    gfb_status st = GFB_OK;
+    for (int it = 0; it < n_steps && !st; ++it) {
+        st = one_step(s, ev);
+        if (st) break;
+        CU(cudaEventSynchronize(ev[3]));
+        float t;
+        CU(cudaEventElapsedTime(&t, ev[0], ev[1]));
+        acc[0] += t;
+        CU(cudaEventElapsedTime(&t, ev[1], ev[2]));
+        acc[1] += t;
+        CU(cudaEventElapsedTime(&t, ev[2], ev[3]));
+        acc[2] += t;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st) return st;
+    if (ms_element) *ms_element += acc[0];
+    if (ms_node) *ms_node += acc[1];
+    if (ms_record) *ms_record += acc[2];
+    return GFB_OK;
+}
+
+gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
+    if (!s || !info) return fail(GFB_ERR_INVALID, "NULL argument");
+    info->n_colour = (int32_t)s->colour_begin.size() - 1;
+    info->n_pml_cell = s->n_pml;
+    info->n_rec_cell = s->n_rec;
+    info->n_field = s->nfld;
+    info->precision = s->prec;
+    info->n_cell = s->n_cell;
+    info->n_node = s->n_node;
+    info->ngll = s->ng;
+    info->device_bytes = s->device_bytes;
+    info->upload_bytes = s->upload_bytes;
+    info->kernel_launches = s->launches;
+    return GFB_OK;
+}
+
+gfb_status gfb_synchronize(gfb_solver* s) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    return GFB_OK;
+}
+
+gfb_status gfb_current_step(const gfb_solver* s, int32_t* step) {
+    if (!s || !step) return fail(GFB_ERR_INVALID, "NULL argument");
+    *step = s->step;
+    return GFB_OK;
+}
+
+gfb_status gfb_get_state(gfb_solver* s, int32_t field, double* u, double* v, double* a) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    const size_t nF = (size_t)s->n_node * s->F;
+    std::vector<double> tmp(nF);
+    auto pick = [&](double* dst) {
+        for (long long g = 0; g < s->n_node; ++g)
+            for (int c = 0; c < 3; ++c) dst[g * 3 + c] = tmp[g * s->F + field * 3 + c];
+    };
+    if (u) {
+        CU(cudaMemcpy(tmp.data(), s->u, nF * 8, cudaMemcpyDeviceToHost));
+        pick(u);
+    }
+    if (v) {
+        CU(cudaMemcpy(tmp.data(), s->v, nF * 8, cudaMemcpyDeviceToHost));
+        pick(v);
+    }
+    if (a) {
+        if (s->prec == GFB_FP64) {
+            CU(cudaMemcpy(tmp.data(), s->a, nF * 8, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> f(nF);
+            CU(cudaMemcpy(f.data(), s->a, nF * 4, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < nF; ++i) tmp[i] = f[i];
+        }
+        pick(a);
+    }
+    return GFB_OK;
+}
+
+gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const double* u, const double* v,
+                         const double* a) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
+    if (step < 0) return fail(GFB_ERR_INVALID, "step must be >= 0");
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    const size_t nF = (size_t)s->n_node * s->F;
+    std::vector<double> tmp(nF);
+    auto put = [&](const double* src, void* dev, bool is_real_float) -> gfb_status {
+        if (is_real_float) {
+            std::vector<float> f(nF);
+            CU(cudaMemcpy(f.data(), dev, nF * 4, cudaMemcpyDeviceToHost));
+            for (long long g = 0; g < s->n_node; ++g)
+                for (int c = 0; c < 3; ++c) f[g * s->F + field * 3 + c] = src ? (float)src[g * 3 + c] : 0.0f;
+            CU(cudaMemcpy(dev, f.data(), nF * 4, cudaMemcpyHostToDevice));
+        } else {
+            CU(cudaMemcpy(tmp.data(), dev, nF * 8, cudaMemcpyDeviceToHost));
+            for (long long g = 0; g < s->n_node; ++g)
+                for (int c = 0; c < 3; ++c) tmp[g * s->F + field * 3 + c] = src ? src[g * 3 + c] : 0.0;
+            CU(cudaMemcpy(dev, tmp.data(), nF * 8, cudaMemcpyHostToDevice));
+        }
+        return GFB_OK;
+    };
+    gfb_status st;
+    if ((st = put(u, s->u, false))) return st;
+    if ((st = put(v, s->v, false))) return st;
+    if ((st = put(a, s->a, s->prec == GFB_FP32))) return st;
+    if (s->has_cpml) {
+        const size_t es = s->prec == GFB_FP64 ? 8 : 4;
+        CU(cudaMemset(s->pml_mem, 0, (size_t)s->n_pml * s->F * 3 * s->nn * es));
+        CU(cudaMemset(s->pml_prev, 0, (size_t)s->n_pml * s->F * s->nn * es));
+    }
+    if ((st = launch_predict(s))) return st;
+    CU(cudaStreamSynchronize(s->stream));
+    s->step = step;
+    return GFB_OK;
+}
+
+gfb_status gfb_records_pending(gfb_solver* s, int32_t* n) {
+    if (!s || !n) return fail(GFB_ERR_INVALID, "NULL argument");
+    *n = (int32_t)s->pending.size();
+    return GFB_OK;
+}
+
+gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* strain, double* u,
+                           double* v, double* a, int32_t release) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
+    if (s->pending.empty()) return fail(GFB_ERR_STATE, "no snapshot pending");
+    CU(cudaSetDevice(s->device));
+    Snapshot& snap = s->pending.front();
+    const size_t per_field = (size_t)s->n_rec * s->nn * 15;
+    std::vector<double> buf(per_field);
+    const double* src;
+    if (snap.slot >= 0) {
+        CU(cudaEventSynchronize(snap.done));
+        CU(cudaMemcpyAsync(buf.data(), s->ring + (size_t)snap.slot * snapshot_doubles(s) + field * per_field,
+                           per_field * 8, cudaMemcpyDeviceToHost, s->copy_stream));
+        CU(cudaStreamSynchronize(s->copy_stream));
+        src = buf.data();
+    } else {
+        src = snap.host.data() + field * per_field;
+    }
+    if (step) *step = snap.step;
+    const size_t npt = (size_t)s->n_rec * s->nn;
+    for (size_t q = 0; q < npt; ++q) {
+        const double* o = src + q * 15;
+        if (strain)
+            for (int c = 0; c < 6; ++c) strain[q * 6 + c] = o[c];
+        for (int c = 0; c < 3; ++c) {
+            if (u) u[q * 3 + c] = o[6 + c];
+            if (v) v[q * 3 + c] = o[9 + c];
+            if (a) a[q * 3 + c] = o[12 + c];
+        }
+    }
+    if (!snap.read_mask[field]) {
+        snap.read_mask[field] = 1;
+        snap.fields_read++;
+    }
+    if (release || snap.fields_read == s->nfld) {
+        if (snap.slot >= 0) s->free_slots.push_back(snap.slot);
+        cudaEventDestroy(snap.done);
+        s->pending.pop_front();
+    }
+    return GFB_OK;
+}
+
+gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const double* jacobian,
+                                const double* lambda_, const double* mu, const double* D,
+                                const double* weights, int32_t ngll, const double* u, double* r,
+                                int32_t precision, int32_t device) {
+    if (n_elem <= 0 || !dxi_dx || !jacobian || !lambda_ || !mu || !u || !r)
+        return fail(GFB_ERR_INVALID, "element residual: missing input");
+    if (ngll < 3 || ngll > 6) return fail(GFB_ERR_UNSUPPORTED, "ngll=%d outside 3..6", ngll);
+    (void)D;
+    (void)weights;  // tables are rebuilt from ngll (same values as gll.hpp)
+    const int nn = ngll * ngll * ngll;
+    const long long P = (long long)n_elem * nn;
+    if (P >= (long long)gfb::kNodeMask) return fail(GFB_ERR_INVALID, "too many element nodes");
+    // independent elements: every element-local point is its own node, one
+    // colour, every point first-touch, so force == element-local residual
+    std::vector<int32_t> ib(P);
+    std::vector<double> mass(P, 1.0);
+    for (long long q = 0; q < P; ++q) ib[q] = (int32_t)q;
+    gfb_mesh m{};
+    m.n_cell = n_elem;
+    m.ngll = ngll;
+    m.n_node = (int32_t)P;
+    m.ibool = ib.data();
+    m.dxi_dx = dxi_dx;
+    m.jacobian = jacobian;
+    m.lambda_ = lambda_;
+    m.mu = mu;
+    m.mass = mass.data();
+    gfb_config c{};
+    c.dt = 1.0;
+    c.precision = precision;
+    c.n_field = 1;
+    c.device = device;
+    c.record_slots = 1;
+    gfb_solver* s = nullptr;
+    gfb_status st = gfb_create(&m, &c, nullptr, &s);
+    if (st) return st;
+    std::unique_ptr<gfb_solver, gfb_status (*)(gfb_solver*)> guard(s, gfb_destroy);
+    const size_t nF = (size_t)P * 3;
+    if (precision == GFB_FP64) {
+        CU(cudaMemcpy(s->ut, u, nF * 8, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(nF);
+        for (size_t i = 0; i < nF; ++i) f[i] = (float)u[i];
+        CU(cudaMemcpy(s->ut, f.data(), nF * 4, cudaMemcpyHostToDevice));
+    }
+    if ((st = launch_elem(s, 0, 0.0))) return st;
+    CU(cudaStreamSynchronize(s->stream));
+    if (precision == GFB_FP64) {
+        CU(cudaMemcpy(r, s->force, nF * 8, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> f(nF);
+        CU(cudaMemcpy(f.data(), s->force, nF * 4, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < nF; ++i) r[i] = f[i];
+    }
+    return GFB_OK;
+}
+
+int32_t gfb_run_forward(const char* direction, int32_t resume, int32_t effective_nprocs) {
+    (void)resume;
+    (void)effective_nprocs;
+    if (!direction || (strcmp(direction, "x") && strcmp(direction, "y") && strcmp(direction, "z"))) {
+        fail(GFB_ERR_INVALID, "--direction must be x, y, or z");
+        return 1;
+    }
+    fail(GFB_ERR_IO, "this build has no HDF5 reader for config.h5 / partition_{r}.h5");
+    return 1;
+}
+
+}  // extern "C"

@@ -1,1 +1,301 @@
-"""gfb -- host-side Python package of the B200 CG-SEM elastic solver."""
+"""gfb -- Python binding of the B200 CG-SEM elastic time loop.
+
+Thin ctypes layer over the C ABI declared in include/gfb.h and implemented
+in lib/libgfb.so (CUDA, sm_100a).  There is no CPU fallback: constructing a
+``Solver`` without the library or without a GPU raises.
+
+Reference interface mirrored: the single-GPU device API of the reference
+forward solver (forward/share/include/gf/cuda_step.hpp:70-129) driven the way
+``run_forward`` drives it (forward/share/src/solver.cpp:389-508).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libgfb.so")
+HEADER_PATH = os.path.join(os.path.dirname(PKG_ROOT), "include", "gfb.h")
+
+FP64, FP32 = 0, 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+class GfbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"gfb status {status}: {message}")
+        self.status = status
+
+
+class Mesh(C.Structure):
+    _fields_ = [
+        ("n_cell", C.c_int32),
+        ("ngll", C.c_int32),
+        ("n_node", C.c_int32),
+        ("ibool", _ip),
+        ("cell_ids", _lp),
+        ("dxi_dx", _dp),
+        ("jacobian", _dp),
+        ("lambda_", _dp),
+        ("mu", _dp),
+        ("density", _dp),
+        ("mass", _dp),
+        ("damping", _dp),
+        ("pml_region", _ip),
+        ("pml_coef_alpha", _dp),
+        ("pml_coef_abar", _dp),
+        ("n_rec_cell", C.c_int32),
+        ("rec_cell_local", _ip),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double),
+        ("snapshot_stride", C.c_int32),
+        ("precision", C.c_int32),
+        ("n_field", C.c_int32),
+        ("field_dir", C.c_int32 * 3),
+        ("device", C.c_int32),
+        ("record_slots", C.c_int32),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("n_colour", C.c_int32),
+        ("n_pml_cell", C.c_int32),
+        ("n_rec_cell", C.c_int32),
+        ("n_field", C.c_int32),
+        ("precision", C.c_int32),
+        ("n_cell", C.c_int32),
+        ("n_node", C.c_int32),
+        ("ngll", C.c_int32),
+        ("device_bytes", C.c_int64),
+        ("upload_bytes", C.c_int64),
+        ("kernel_launches", C.c_int64),
+    ]
+
+
+class Source(C.Structure):
+    _fields_ = [
+        ("n_src_cell", C.c_int32),
+        ("cell_ids", _lp),
+        ("weights", _dp),
+        ("n_stf", C.c_int32),
+        ("stf", _dp),
+    ]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load lib/libgfb.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: build it with `make -C gf-only-sem_b200`")
+    lib = C.CDLL(path)
+    lib.gfb_abi_version.restype = C.c_int32
+    lib.gfb_last_error.restype = C.c_char_p
+    lib.gfb_create.argtypes = [C.POINTER(Mesh), C.POINTER(Config), C.POINTER(Source), C.POINTER(C.c_void_p)]
+    lib.gfb_destroy.argtypes = [C.c_void_p]
+    lib.gfb_advance.argtypes = [C.c_void_p, C.c_int32]
+    lib.gfb_synchronize.argtypes = [C.c_void_p]
+    lib.gfb_advance_profiled.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
+    lib.gfb_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
+    lib.gfb_current_step.argtypes = [C.c_void_p, _ip]
+    lib.gfb_get_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
+    lib.gfb_set_state.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp, _dp]
+    lib.gfb_records_pending.argtypes = [C.c_void_p, _ip]
+    lib.gfb_read_record.argtypes = [C.c_void_p, C.c_int32, _ip, _dp, _dp, _dp, _dp, C.c_int32]
+    lib.gfb_element_residual.argtypes = [C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int32, _dp, _dp, C.c_int32, C.c_int32]
+    lib.gfb_run_forward.argtypes = [C.c_char_p, C.c_int32, C.c_int32]
+    lib.gfb_run_forward.restype = C.c_int32
+    for name in (
+        "gfb_create", "gfb_destroy", "gfb_advance", "gfb_synchronize", "gfb_current_step",
+        "gfb_get_state", "gfb_set_state", "gfb_records_pending", "gfb_read_record",
+        "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info",
+    ):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(st: int):
+    if st != 0:
+        raise GfbError(st, load_library().gfb_last_error().decode())
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return C.cast(None, C.POINTER(ctype))
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def element_residual(dxi_dx, jacobian, lam, mu, u, ngll: int, precision: int = FP64, device: int = 0):
+    """K_e u for independent elements on the GPU (compute_element_residual<BackendCUDA>)."""
+    lib = load_library()
+    nn = ngll**3
+    arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (dxi_dx, jacobian, lam, mu, u)]
+    n_elem = arrs[1].size // nn
+    r = np.zeros(n_elem * nn * 3)
+    _check(
+        lib.gfb_element_residual(
+            n_elem, *[_ptr(a, C.c_double) for a in arrs[:4]], None, None, ngll,
+            _ptr(arrs[4], C.c_double), _ptr(r, C.c_double), precision, device
+        )
+    )
+    return r
+
+
+class Solver:
+    """All wavefields of one model advanced together on one GPU.
+
+    ``prob`` is a dict of reference-layout arrays (see gfb.mesh.build_problem);
+    ``dirs`` lists the force direction (0=x, 1=y, 2=z) of each wavefield.
+    """
+
+    def __init__(self, prob: dict, dirs: Sequence[int] = (0,), precision: int = FP64,
+                 device: int = 0, record_slots: int = 4, record: bool = True):
+        self.lib = load_library()
+        keep = {}
+
+        def arr(name, dtype):
+            if name not in prob or prob[name] is None:
+                return None
+            a = np.ascontiguousarray(prob[name], dtype=dtype).ravel()
+            keep[name] = a
+            return a
+
+        m = Mesh()
+        m.n_cell = int(prob["n_cell"])
+        m.ngll = int(prob["ngll"])
+        m.n_node = int(prob["n_node"])
+        m.ibool = _ptr(arr("ibool", np.int32), C.c_int32)
+        m.cell_ids = _ptr(arr("cell_ids", np.int64), C.c_int64)
+        m.dxi_dx = _ptr(arr("dxi_dx", np.float64), C.c_double)
+        m.jacobian = _ptr(arr("jacobian", np.float64), C.c_double)
+        m.lambda_ = _ptr(arr("lambda", np.float64), C.c_double)
+        m.mu = _ptr(arr("mu", np.float64), C.c_double)
+        m.density = _ptr(arr("density", np.float64), C.c_double)
+        m.mass = _ptr(arr("mass", np.float64), C.c_double)
+        m.damping = _ptr(arr("damping", np.float64), C.c_double)
+        m.pml_region = _ptr(arr("pml_region", np.int32), C.c_int32)
+        m.pml_coef_alpha = _ptr(arr("pml_coef_alpha", np.float64), C.c_double)
+        m.pml_coef_abar = _ptr(arr("pml_coef_abar", np.float64), C.c_double)
+        rec = prob.get("recording") if record else None
+        if rec is not None:
+            rc = np.ascontiguousarray(rec["rec_cell_local"], dtype=np.int32)
+            keep["rec"] = rc
+            m.n_rec_cell = int(rc.size)
+            m.rec_cell_local = _ptr(rc, C.c_int32)
+        else:
+            m.n_rec_cell = 0
+            m.rec_cell_local = _ptr(None, C.c_int32)
+        c = Config()
+        c.dt = float(prob["dt"])
+        c.snapshot_stride = int(prob.get("snapshot_stride", 0))
+        c.precision = int(precision)
+        c.n_field = len(dirs)
+        for i, d in enumerate(dirs):
+            c.field_dir[i] = int(d)
+        c.device = int(device)
+        c.record_slots = int(record_slots)
+        s = Source()
+        ids = arr("src_cell_ids", np.int64)
+        s.n_src_cell = 0 if ids is None else int(ids.size)
+        s.cell_ids = _ptr(ids, C.c_int64)
+        s.weights = _ptr(arr("src_weights", np.float64), C.c_double)
+        stf = arr("stf", np.float64)
+        s.n_stf = 0 if stf is None else int(stf.size)
+        s.stf = _ptr(stf, C.c_double)
+        h = C.c_void_p()
+        _check(self.lib.gfb_create(C.byref(m), C.byref(c), C.byref(s), C.byref(h)))
+        self.h = h
+        self.n_node = m.n_node
+        self.n_field = len(dirs)
+        self.n_rec = m.n_rec_cell
+        self.nn = m.ngll**3
+        del keep
+
+    def advance(self, n_steps: int):
+        _check(self.lib.gfb_advance(self.h, int(n_steps)))
+
+    def advance_profiled(self, n_steps: int):
+        """Advance and return device milliseconds per phase (element, node, record)."""
+        t = [C.c_double(0.0) for _ in range(3)]
+        _check(self.lib.gfb_advance_profiled(self.h, int(n_steps), *[C.byref(x) for x in t]))
+        return tuple(x.value for x in t)
+
+    def info(self) -> dict:
+        i = Info()
+        _check(self.lib.gfb_get_info(self.h, C.byref(i)))
+        return {name: getattr(i, name) for name, _ in Info._fields_}
+
+    def synchronize(self):
+        _check(self.lib.gfb_synchronize(self.h))
+
+    @property
+    def step(self) -> int:
+        s = C.c_int32()
+        _check(self.lib.gfb_current_step(self.h, C.byref(s)))
+        return s.value
+
+    def state(self, field: int = 0):
+        u, v, a = (np.zeros(self.n_node * 3) for _ in range(3))
+        _check(self.lib.gfb_get_state(self.h, field, _ptr(u, C.c_double), _ptr(v, C.c_double), _ptr(a, C.c_double)))
+        return u.reshape(-1, 3), v.reshape(-1, 3), a.reshape(-1, 3)
+
+    def set_state(self, field: int, step: int, u=None, v=None, a=None):
+        cv = [None if x is None else np.ascontiguousarray(x, dtype=np.float64).ravel() for x in (u, v, a)]
+        _check(self.lib.gfb_set_state(self.h, field, step, *[_ptr(x, C.c_double) for x in cv]))
+
+    def pending(self) -> int:
+        n = C.c_int32()
+        _check(self.lib.gfb_records_pending(self.h, C.byref(n)))
+        return n.value
+
+    def read_record(self, field: int = 0, release: bool = False):
+        step = C.c_int32()
+        strain = np.zeros((self.n_rec, self.nn, 6))
+        u, v, a = (np.zeros((self.n_rec, self.nn, 3)) for _ in range(3))
+        _check(self.lib.gfb_read_record(self.h, field, C.byref(step), _ptr(strain, C.c_double),
+                                        _ptr(u, C.c_double), _ptr(v, C.c_double), _ptr(a, C.c_double),
+                                        1 if release else 0))
+        return {"step": step.value, "strain": strain, "u": u, "v": v, "a": a}
+
+    def drain(self):
+        """All pending snapshots as {field: dict of stacked arrays}."""
+        out = {f: {"steps": [], "strain": [], "u": [], "v": [], "a": []} for f in range(self.n_field)}
+        while self.pending() > 0:
+            for f in range(self.n_field):
+                r = self.read_record(f)
+                out[f]["steps"].append(r["step"])
+                for k in ("strain", "u", "v", "a"):
+                    out[f][k].append(r[k])
+        for f in out:
+            for k in out[f]:
+                out[f][k] = np.array(out[f][k])
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gfb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

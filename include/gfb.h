@@ -1,0 +1,217 @@
+/*
+ * gfb.h -- C ABI of the B200 (sm_100a) CG-SEM elastic time loop.
+ *
+ * Drop-in boundary for the path that `gf_solver_elastic_cuda --direction
+ * {x,y,z}` runs in changguo1998/GF-only-SEM.  The reference binds this path
+ * through C++ only: `int gf::run_forward(const std::string&, bool, int)`
+ * (forward/share/include/gf/solver.hpp:21) over the device API of
+ * forward/share/include/gf/cuda_step.hpp:70-129 and the element kernel
+ * entry `compute_element_residual<BackendCUDA>` (forward/share/include/gf/
+ * element.hpp:39-42).  Each entry point below names the reference interface
+ * it replaces.
+ *
+ * Conventions
+ *  - Plain pointers and sizes; no C++ or torch types cross the boundary.
+ *  - Every function returns a gfb_status; GFB_OK == 0.  A failing call
+ *    leaves a message retrievable with gfb_last_error() (per thread).
+ *    Nothing aborts the process (the reference aborts in GF_CUDA_CHECK,
+ *    forward/share/include/gf/cuda_check.h:16-24).
+ *  - Host arrays passed to gfb_create are read during the call only.
+ *  - Array layouts are the reference's (RankData, forward/share/include/gf/
+ *    types.hpp:27-140): element-major, GLL node (i*ngll + j)*ngll + k,
+ *    components last.
+ */
+#ifndef GFB_H
+#define GFB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFB_ABI_VERSION 1
+
+typedef enum gfb_status {
+    GFB_OK = 0,
+    GFB_ERR_INVALID = 1,    /* bad argument or inconsistent mesh            */
+    GFB_ERR_CUDA = 2,       /* CUDA runtime error (message has the detail)  */
+    GFB_ERR_NOMEM = 3,      /* device or host allocation failed             */
+    GFB_ERR_STATE = 4,      /* call not valid in the solver's current state */
+    GFB_ERR_UNSUPPORTED = 5,/* e.g. polynomial order outside 2..5           */
+    GFB_ERR_NO_DEVICE = 6,  /* no CUDA device (reference main.cpp:51-58)    */
+    GFB_ERR_IO = 7          /* file input/output failure                    */
+} gfb_status;
+
+typedef enum gfb_precision {
+    GFB_FP64 = 0, /* all arithmetic in FP64 (parity path, 1e-10 vs oracle)         */
+    GFB_FP32 = 1  /* FP32 element/C-PML arithmetic, FP64 displacement & velocity  */
+} gfb_precision;
+
+/*
+ * Merged partition set (the result of read_partition_all,
+ * forward/share/src/io.cpp:319-450).  n_node is n_rank_node.
+ */
+typedef struct gfb_mesh {
+    int32_t n_cell;            /* number of hexahedral cells                   */
+    int32_t ngll;              /* N+1, 3..6 supported                          */
+    int32_t n_node;            /* unique GLL nodes (max(ibool)+1)              */
+    const int32_t* ibool;      /* [n_cell*ngll^3] local_cell2rank_node         */
+    const int64_t* cell_ids;   /* [n_cell] local_cell_ids; NULL -> 0..n-1      */
+    const double* dxi_dx;      /* [n_cell*ngll^3*9]                            */
+    const double* jacobian;    /* [n_cell*ngll^3] det J                        */
+    const double* lambda_;     /* [n_cell*ngll^3]                              */
+    const double* mu;          /* [n_cell*ngll^3]                              */
+    const double* density;     /* [n_cell*ngll^3] (read only with C-PML)       */
+    const double* mass;        /* [n_cell*ngll^3] element-local lumped mass    */
+    const double* damping;     /* [n_cell*ngll^3] legacy ramp; NULL -> none    */
+    const int32_t* pml_region; /* [n_cell] 0 interior, 1..7 C-PML region       */
+    const double* pml_coef_alpha; /* [n_cell*ngll^3*9]                         */
+    const double* pml_coef_abar;  /* [n_cell*ngll^3*5]; NULL -> no C-PML       */
+    int32_t n_rec_cell;        /* recording cells (0 -> no snapshots)          */
+    const int32_t* rec_cell_local; /* [n_rec_cell] merged local cell index     */
+} gfb_mesh;
+
+/* Time-loop configuration (ConfigData, types.hpp:128-140, subset). */
+typedef struct gfb_config {
+    double dt;                 /* solver_dt                                    */
+    int32_t snapshot_stride;   /* record when step % stride == 0; <=0 never    */
+    int32_t precision;         /* gfb_precision                                */
+    int32_t n_field;           /* wavefields advanced together, 1..3           */
+    int32_t field_dir[3];      /* force direction per wavefield, 0=x 1=y 2=z   */
+    int32_t device;            /* CUDA device ordinal                          */
+    int32_t record_slots;      /* snapshot slots kept on the device (>=1)      */
+} gfb_config;
+
+/* Point-force source (config.h5 /source, io.cpp:681-707). */
+typedef struct gfb_source {
+    int32_t n_src_cell;        /* containing cells                             */
+    const int64_t* cell_ids;   /* [n_src_cell] matched against mesh cell_ids   */
+    const double* weights;     /* [n_src_cell*ngll^3] Lagrange weights         */
+    int32_t n_stf;             /* samples of the source time function          */
+    const double* stf;         /* [n_stf] stf_values; step s uses stf[s]       */
+} gfb_source;
+
+typedef struct gfb_solver gfb_solver;
+
+/* ABI version of the loaded library (compare with GFB_ABI_VERSION). */
+int32_t gfb_abi_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* gfb_last_error(void);
+
+/*
+ * Build a solver on the GPU: validate the mesh, assemble the global lumped
+ * mass / damping (solver.cpp:188-217), initialise C-PML memory
+ * (pml.cpp:41-53), map source cells (solver.cpp:247-261), colour the cells
+ * for atomic-free assembly and upload everything.
+ * Replaces cuda_allocate_state (cuda_step.hpp:70-78) and the set-up part of
+ * run_forward (solver.cpp:100-276).
+ */
+gfb_status gfb_create(const gfb_mesh* mesh, const gfb_config* config, const gfb_source* source,
+                      gfb_solver** out);
+
+/* Release all device and host memory.  Replaces cuda_free_state
+ * (cuda_step.hpp:80-81). */
+gfb_status gfb_destroy(gfb_solver* solver);
+
+/*
+ * Advance n_steps solver steps for all wavefields.  One step is the sequence
+ * of run_forward's loop body (solver.cpp:389-444 on the GPU, 510-622 on the
+ * CPU): Newmark predictor, gather, element internal force, C-PML or legacy
+ * damping, source injection, assembly, corrector, C-PML memory update; at
+ * steps with step % stride == 0 a snapshot of the recording cells is stored
+ * in the device ring (solver.cpp:454-507).
+ * Replaces cuda_newmark_predict, cuda_gather_predicted, cuda_zero_residual,
+ * cuda_launch_element_residual, cuda_pml_damping, cuda_source_injection,
+ * cuda_scatter_to_rank and cuda_newmark_correct (cuda_step.hpp:87-117).
+ * Returns GFB_ERR_STATE if un-read snapshots would be overwritten.
+ */
+gfb_status gfb_advance(gfb_solver* solver, int32_t n_steps);
+
+/*
+ * gfb_advance with CUDA events on the solver's stream around each phase of
+ * every step; adds the device milliseconds spent in the element/assembly
+ * launches, the node update and the snapshot kernel to the three outputs
+ * (any may be NULL).  Synchronises before returning.  The reference times
+ * its loop with std::chrono only (solver.cpp:342-348, 729-732).
+ */
+gfb_status gfb_advance_profiled(gfb_solver* solver, int32_t n_steps, double* ms_element,
+                                double* ms_node, double* ms_record);
+
+/* Static description of a solver and its cumulative kernel-launch count. */
+typedef struct gfb_info {
+    int32_t n_colour;        /* assembly colours (launches of the element kernel per step) */
+    int32_t n_pml_cell;      /* cells with C-PML state                                      */
+    int32_t n_rec_cell;
+    int32_t n_field;
+    int32_t precision;
+    int32_t n_cell;
+    int32_t n_node;
+    int32_t ngll;
+    int64_t device_bytes;    /* device memory held                                         */
+    int64_t upload_bytes;    /* bytes copied host->device by gfb_create                    */
+    int64_t kernel_launches; /* kernels launched by this solver so far                     */
+} gfb_info;
+
+gfb_status gfb_get_info(const gfb_solver* solver, gfb_info* info);
+
+/* Wait for all queued work. */
+gfb_status gfb_synchronize(gfb_solver* solver);
+
+/* Next solver step index (number of steps taken since step 0). */
+gfb_status gfb_current_step(const gfb_solver* solver, int32_t* step);
+
+/*
+ * Copy the global state of wavefield `field` to host arrays of n_node*3
+ * doubles (any may be NULL).  Replaces cuda_copy_state_to_host
+ * (cuda_step.hpp:103-105).
+ */
+gfb_status gfb_get_state(gfb_solver* solver, int32_t field, double* u, double* v, double* a);
+
+/*
+ * Overwrite the global state of wavefield `field` and set the step counter
+ * (resume from a restart file, solver.cpp:369-388).  C-PML memory is reset
+ * to zero, as the reference restart does not store it (restart.cpp:120-152).
+ */
+gfb_status gfb_set_state(gfb_solver* solver, int32_t field, int32_t step, const double* u,
+                         const double* v, const double* a);
+
+/* Number of snapshots waiting to be read. */
+gfb_status gfb_records_pending(gfb_solver* solver, int32_t* n);
+
+/*
+ * Pop the oldest snapshot of wavefield `field` into host buffers laid out as
+ * the record datasets of RecordWriter::write_step (record.cpp:175-257)
+ * without the leading unit axis:
+ *   strain [n_rec_cell, ngll^3, 6] (xx,yy,zz,xy,xz,yz)
+ *   u, v, a [n_rec_cell, ngll^3, 3]
+ * Any buffer may be NULL.  The snapshot is released once every wavefield
+ * has been read (or immediately when release != 0).
+ */
+gfb_status gfb_read_record(gfb_solver* solver, int32_t field, int32_t* step, double* strain,
+                           double* u, double* v, double* a, int32_t release);
+
+/*
+ * Element internal force for n_elem independent elements, host arrays in
+ * and out (r is overwritten with K_e u).  Replaces
+ * compute_element_residual<BackendCUDA> (element.hpp:39-42,
+ * element_cuda.cu:195-252); D and weights are the GLL tables of ngll.
+ * precision selects the FP64 or FP32 kernel.
+ */
+gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const double* jacobian,
+                                const double* lambda_, const double* mu, const double* D,
+                                const double* weights, int32_t ngll, const double* u, double* r,
+                                int32_t precision, int32_t device);
+
+/*
+ * File-level driver: run the forward solve of one direction with the
+ * reference's CWD-relative file contract (solver.cpp:73-739,
+ * main.cpp:32-137).  Returns 0 on success, 1 on failure, like run_forward.
+ */
+int32_t gfb_run_forward(const char* direction, int32_t resume, int32_t effective_nprocs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFB_H */

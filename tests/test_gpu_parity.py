@@ -1,0 +1,194 @@
+"""GPU parity tests: the CUDA path through the C ABI against the CPU oracle.
+
+Tolerances (stated by the spec of this path):
+  * FP64 path: relative L2 <= 1e-10 on recorded traces and final state;
+    element kernel max relative difference <= 1e-12
+    (the reference's own CUDA-vs-CPU bound, tests/test_element_cuda.cu:99-136);
+  * FP32 batched path: relative L2 <= 1e-4 against the FP64 oracle.
+Integer/map outputs (snapshot step indices) are compared exactly.
+"""
+
+import numpy as np
+import pytest
+from conftest import golden_cases, golden_problem, load_golden, rel_l2
+
+import gfb
+import oracle
+from gfb import mesh
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 1e-4
+
+
+def random_elements(ngll, n_elem, seed):
+    """Random elements by the rules of tests/test_element_cuda.cu:35-95."""
+    rng = np.random.default_rng(seed)
+    nn = ngll**3
+    P = n_elem * nn
+    dxi = rng.uniform(-1, 1, (P, 9))
+    dxi[:, 0] += 3.0
+    dxi[:, 4] += 3.0
+    dxi[:, 8] += 3.0
+    jac = np.abs(rng.uniform(-1, 1, P)) + 0.01
+    vp = np.abs(rng.uniform(-1, 1, P)) + 1000.0
+    vs = np.abs(rng.uniform(-1, 1, P)) + 500.0
+    rho = np.abs(rng.uniform(-1, 1, P)) + 1000.0
+    mu = rho * vs * vs
+    lam = rho * (vp * vp - 2.0 * vs * vs)
+    u = rng.uniform(-1, 1, (P, 3))
+    return dxi, jac, lam, mu, u
+
+
+@pytest.mark.parametrize("ngll", [3, 4, 5, 6])
+def test_element_kernel_fp64_matches_oracle(ngll):
+    dxi, jac, lam, mu, u = random_elements(ngll, 7, 123 + ngll)
+    ref = oracle.element_residual(dxi, jac, lam, mu, u, ngll)
+    got = gfb.element_residual(dxi, jac, lam, mu, u, ngll, gfb.FP64)
+    rel = np.abs(got - ref).max() / np.abs(ref).max()
+    assert rel < 1e-12, rel
+
+
+@pytest.mark.parametrize("ngll", [4, 5])
+def test_element_kernel_fp32_and_rigid_translation(ngll):
+    dxi, jac, lam, mu, u = random_elements(ngll, 5, 7)
+    ref = oracle.element_residual(dxi, jac, lam, mu, u, ngll)
+    got = gfb.element_residual(dxi, jac, lam, mu, u, ngll, gfb.FP32)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-5
+    # rigid translation gives a zero residual (tests/test_element_cuda.cu:168-187)
+    ut = np.tile([1.0, -2.0, 0.5], (u.shape[0], 1))
+    r = gfb.element_residual(dxi, jac, lam, mu, ut, ngll, gfb.FP64)
+    scale = np.abs(gfb.element_residual(dxi, jac, lam, mu, u, ngll, gfb.FP64)).max()
+    assert np.abs(r).max() < 1e-10 * scale
+
+
+def compare_runs(gpu_snaps, orc_snaps, tol, what=""):
+    np.testing.assert_array_equal(np.asarray(gpu_snaps["steps"]), orc_snaps["steps"])
+    for k in ("strain", "u", "v", "a"):
+        e = rel_l2(gpu_snaps[k], orc_snaps[k])
+        assert e <= tol, f"{what} {k}: rel L2 {e:.3e} > {tol}"
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_time_loop_fp64_matches_golden_traces(name):
+    g = load_golden(name)
+    prob = golden_problem(g)
+    for d in g["dirs"]:
+        s = gfb.Solver(prob, dirs=[int(d)], precision=gfb.FP64)
+        s.advance(int(g["nsteps"]))
+        snaps = s.drain()[0]
+        gold = {k: g[f"trace_{k}_{d}"] for k in ("strain", "u", "v", "a")}
+        gold["steps"] = g[f"trace_steps_{d}"]
+        compare_runs(snaps, gold, FP64_TOL, f"{name} dir {d}")
+        u, v, a = s.state(0)
+        assert rel_l2(u, g[f"final_u_{d}"]) <= FP64_TOL
+        assert rel_l2(v, g[f"final_v_{d}"]) <= FP64_TOL
+        assert rel_l2(a, g[f"final_a_{d}"]) <= FP64_TOL
+        s.close()
+
+
+def layered_problem(nsteps=120, jitter=0.08, order=4, cpml=True, seed=5):
+    spec = mesh.MeshSpec(nx=6, ny=5, nz=4, dx=500.0, dy=500.0, dz=500.0, order=order, jitter=jitter, seed=seed,
+                         pml={"xmin": 1, "xmax": 1, "ymin": 1, "ymax": 1, "zmax": 1})
+    mat = mesh.layered([600.0, 1300.0], [3500.0, 5000.0, 6500.0], [2000.0, 2900.0, 3700.0], [2300.0, 2550.0, 2800.0])
+    return mesh.build_problem(spec, mat, np.array([1430.0, 1270.0, 620.0]), nsteps=nsteps, snapshot_stride=10,
+                              record_depth_max_m=500.0, with_cpml=cpml)
+
+
+def oracle_snaps(prob, d, nsteps):
+    run = oracle.Run(prob, d, "oracle", threads=4)
+    snaps = run.advance(nsteps)
+    return snaps, run.state()
+
+
+def test_three_wavefields_fp64_match_three_oracle_runs():
+    prob = layered_problem()
+    n = prob["nsteps"]
+    s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP64)
+    s.advance(n)
+    snaps = s.drain()
+    for d in range(3):
+        ref, (u, v, a) = oracle_snaps(prob, d, n)
+        compare_runs(snaps[d], ref, FP64_TOL, f"field {d}")
+        gu, gv, ga = s.state(d)
+        assert rel_l2(gu, u) <= FP64_TOL and rel_l2(gv, v) <= FP64_TOL and rel_l2(ga, a) <= FP64_TOL
+
+
+def test_fp32_batched_within_1e4_of_fp64_oracle():
+    prob = layered_problem(nsteps=300)
+    n = prob["nsteps"]
+    s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32)
+    s.advance(n)
+    snaps = s.drain()
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(snaps[d], ref, FP32_TOL, f"fp32 field {d}")
+
+
+@pytest.mark.parametrize("prec", [gfb.FP64, gfb.FP32])
+def test_assembly_is_bit_reproducible(prec):
+    prob = layered_problem(nsteps=60)
+    out = []
+    for _ in range(2):
+        s = gfb.Solver(prob, dirs=[0, 2], precision=prec)
+        s.advance(60)
+        out.append((s.drain(), s.state(1)))
+        s.close()
+    (a, sa), (b, sb) = out
+    for f in (0, 1):
+        for k in ("strain", "u", "v", "a"):
+            np.testing.assert_array_equal(a[f][k], b[f][k])
+    for x, y in zip(sa, sb):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("order", [2, 3, 5])
+def test_other_polynomial_orders_fp64(order):
+    prob = layered_problem(nsteps=50, order=order)
+    s = gfb.Solver(prob, dirs=[1], precision=gfb.FP64)
+    s.advance(50)
+    ref, (u, v, a) = oracle_snaps(prob, 1, 50)
+    compare_runs(s.drain()[0], ref, FP64_TOL, f"order {order}")
+
+
+def test_edge_cases_fp64():
+    """Legacy ramp damping (no C-PML), mu <= 0 nodes skipped
+    (element_cpu.cpp:42-43), a zero-mass node held at a = 0
+    (solver.cpp:58-61), an STF shorter than the run (solver.cpp:579-582) and a
+    source cell absent from the mesh (solver.cpp:584-587)."""
+    prob = layered_problem(nsteps=80, cpml=False)
+    assert prob["damping"].max() > 0
+    mu = prob["mu"].copy()
+    mu.reshape(prob["n_cell"], -1)[7, :11] = 0.0
+    prob["mu"] = mu
+    mass = prob["mass"].copy().reshape(prob["n_cell"], -1)
+    ib = prob["ibool"].reshape(prob["n_cell"], -1)
+    g0 = ib[3, 62]
+    mass[ib == g0] = 0.0
+    prob["mass"] = mass
+    prob["stf"] = prob["stf"][:55]
+    prob["src_cell_ids"] = np.concatenate([prob["src_cell_ids"], [10**9]])
+    prob["src_weights"] = np.concatenate([prob["src_weights"], prob["src_weights"][:1]])
+    s = gfb.Solver(prob, dirs=[2], precision=gfb.FP64)
+    s.advance(80)
+    ref, (u, v, a) = oracle_snaps(prob, 2, 80)
+    compare_runs(s.drain()[0], ref, FP64_TOL, "edge")
+    gu, gv, ga = s.state(0)
+    assert rel_l2(gu, u) <= FP64_TOL and rel_l2(gv, v) <= FP64_TOL
+    assert np.all(ga[g0] == 0.0)
+
+
+def test_resume_from_state_matches_uninterrupted_run():
+    prob = layered_problem(nsteps=90, cpml=False)
+    full = gfb.Solver(prob, dirs=[0], precision=gfb.FP64, record=False)
+    full.advance(90)
+    first = gfb.Solver(prob, dirs=[0], precision=gfb.FP64, record=False)
+    first.advance(40)
+    u, v, a = first.state(0)
+    second = gfb.Solver(prob, dirs=[0], precision=gfb.FP64, record=False)
+    second.set_state(0, 40, u, v, a)
+    assert second.step == 40
+    second.advance(50)
+    for x, y in zip(second.state(0), full.state(0)):
+        np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-12 * np.abs(y).max())
