@@ -45,6 +45,10 @@ WORKLOADS = {
     # layered model, three directions batched
     "layered_64x64x32": dict(nx=64, ny=64, nz=32, d=250.0, pml=4, seed=2, src=(8000.0, 8000.0, 2000.0),
                              nsteps=4000, stride=10, depth=250.0),
+    # the same model at 40 x 40 x 20 cells: inputs still larger than L2 but
+    # about 1 GB on the device, for ncu captures
+    "layered_40x40x20": dict(nx=40, ny=40, nz=20, d=400.0, pml=4, seed=2, src=(8000.0, 8000.0, 2000.0),
+                             nsteps=2500, stride=10, depth=400.0),
     # configs[0]-shaped halfspace (CPU-runnable size) for quick runs
     "halfspace_20x20x10": dict(nx=20, ny=20, nz=10, d=500.0, pml=3, seed=0, src=(5000.0, 5000.0, 1000.0),
                                nsteps=2000, stride=10, depth=500.0),
