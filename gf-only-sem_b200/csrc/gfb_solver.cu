@@ -986,3 +986,15 @@ int32_t gfb_run_forward(const char* direction, int32_t resume, int32_t effective
 }
 
 }  // extern "C"
+
+// Internal hooks shared with other translation units of this library.
+namespace gfb {
+
+gfb_status set_error(gfb_status st, const char* msg) { return fail(st, "%s", msg); }
+
+bool gll_tables_for(int ngll, std::vector<double>& w, std::vector<double>& D) {
+    std::vector<double> x;
+    return gll_tables(ngll - 1, x, w, D);
+}
+
+}  // namespace gfb

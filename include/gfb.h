@@ -205,6 +205,37 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
                                 int32_t precision, int32_t device);
 
 /*
+ * Element internal force that allocates nothing.  No counterpart in the
+ * reference.
+ *
+ * For callers that cannot call cudaMalloc: code whose device memory is all
+ * owned by a caching pool or a host framework (allocating behind it
+ * fragments the pool and can fail under memory pressure), code that cannot
+ * afford the implicit device synchronisation of cudaMalloc/cudaFree inside
+ * its loop, and code running where the allocator is intercepted.  The
+ * caller passes DEVICE pointers, in the layouts of gfb_element_residual:
+ * dxi_dx [n_elem*ngll^3*9], jacobian, lambda_, mu [n_elem*ngll^3],
+ * u [n_elem*ngll^3*3] in, r [n_elem*ngll^3*3] out (overwritten with K_e u).
+ * Work is queued on `stream` (a cudaStream_t; NULL = legacy default stream)
+ * of the current device; the call does not wait for it.
+ *
+ * The kernel's scratch (cell geometry repacked for the kernel, the node
+ * table and the derivative table) lives in one fixed 8 MiB device array
+ * inside the library; every GPU that loads the library holds it until the
+ * process exits.  n_elem is limited to what fits: 3106 cells at ngll=3,
+ * 1310 at ngll=4, 671 at ngll=5, 388 at ngll=6; larger calls are rejected
+ * with GFB_ERR_INVALID and a message giving the maximum (split the call).
+ * The first call on a device looks up the array's device address; make
+ * that first call before any CUDA stream capture.  All calls on a device
+ * share the one array and each call rewrites the part it reads, so calls
+ * that may overlap on the GPU (different streams, or host threads without
+ * ordering) race; serialise them on one stream.  FP64 only.
+ */
+gfb_status gfb_element_residual_noalloc(int32_t n_elem, const double* dxi_dx, const double* jacobian,
+                                        const double* lambda_, const double* mu, int32_t ngll,
+                                        const double* u, double* r, void* stream);
+
+/*
  * File-level driver: run the forward solve of one direction with the
  * reference's CWD-relative file contract (solver.cpp:73-739,
  * main.cpp:32-137).  Returns 0 on success, 1 on failure, like run_forward.
