@@ -141,8 +141,32 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def node_pml_live_axes(prob):
+    """Per global node: number of C-PML memory axes with a nonzero assembled
+    coefficient (the node form keeps and updates only those)."""
+    from gfb import mesh as gmesh
+
+    nc, nn = prob["n_cell"], 125
+    cells = np.nonzero(prob["pml_region"])[0]
+    A = prob["pml_coef_abar"].reshape(nc, nn, 5)[cells]
+    w = gmesh.gll_weights(gmesh.gll_points(4))
+    wg = (w[:, None, None] * w[None, :, None] * w[None, None, :]).ravel()
+    rho = prob["density"].reshape(nc, nn)[cells]
+    jac = prob["jacobian"].reshape(nc, nn)[cells]
+    scale = wg[None, :] * np.where(rho > 0, 1.0 / rho, 0.0) * jac
+    ib = prob["ibool"].reshape(nc, nn)[cells]
+    B = np.zeros((prob["n_node"], 5))
+    for k in range(5):
+        np.add.at(B[:, k], ib.ravel(), (scale * A[:, :, k]).ravel())
+    has = np.zeros(prob["n_node"], dtype=bool)
+    has[ib.ravel()[np.any(A != 0, axis=2).ravel()]] = True
+    return int(has.sum()), int((B[:, 2:] != 0).sum())
+
+
 def elem_bytes_per_step(prob, info, n_field, prec):
-    """Algorithmic DRAM bytes of one step's element/assembly launches."""
+    """Algorithmic DRAM bytes of one step's element/assembly launches
+    (unpadded component bytes; the [node][field][4] layout moves 4/3 of the
+    gather/force bytes, visible in the ncu traffic)."""
     nn = 125
     P = prob["n_cell"] * nn
     G = prob["n_node"]
@@ -151,15 +175,21 @@ def elem_bytes_per_step(prob, info, n_field, prec):
     geom = P * 12 * sr + P * 4                      # geometry + ibool
     gather = P * F * sr                              # predicted displacement
     force = G * F * sr + (P - G) * F * sr * 2        # first touch writes, others read+write
-    Ppml = info["n_pml_cell"] * nn
-    pml = Ppml * (15 * sr + F * 3 * sr * 2 + F * sr * 2 + F * 16 + F * sr)
+    pml = 0
+    if info["n_pml_node"] == 0:                      # per-cell C-PML in this kernel
+        Ppml = info["n_pml_cell"] * nn
+        pml = Ppml * (15 * sr + F * 3 * sr * 2 + F * sr * 2 + F * 16 + F * sr)
     return geom + gather + force + pml
 
 
-def node_bytes_per_step(prob, n_field, prec):
+def node_bytes_per_step(prob, info, n_field, prec):
     sr = 4 if prec == 1 else 8
     F = 3 * n_field
-    return prob["n_node"] * (F * (32 + 2 * sr + sr + sr) + 8 + (4 if prec == 1 else 0))
+    base = prob["n_node"] * (F * (32 + 2 * sr + sr + sr) + 8 + (4 if prec == 1 else 0))
+    if info["n_pml_node"] > 0:                       # node-form C-PML in this kernel
+        n_pml, live = node_pml_live_axes(prob)
+        base += n_pml * (4 + 14 * sr + F * sr * 2) + live * F * sr * 2
+    return base
 
 
 def committed_traffic():
@@ -192,6 +222,41 @@ def cpu_baseline_sample(prob, seconds_target=20.0):
     return {"value": val, "unit": UNIT, "cores": threads, "kind": "reference" if which == "ref" else "port",
             "sample": f"{n} FP64 solver steps of direction x on the full mesh after 1 warm-up step "
                       f"({dt:.1f} s; reference element kernel threaded over cells, rest serial)"}
+
+
+class RecordConsumer(threading.Thread):
+    """Reads snapshots while the solver steps, as a record-writer thread of
+    an application would (into reused buffers; the data is not kept)."""
+
+    def __init__(self, solver):
+        super().__init__(daemon=True)
+        self.s = solver
+        self.halt = threading.Event()
+        self.count = 0
+        n = solver.n_rec * solver.nn
+        self.bufs = [np.zeros(n * 6), np.zeros(n * 3), np.zeros(n * 3), np.zeros(n * 3)]
+
+    def _read_all(self):
+        import ctypes as C
+
+        import gfb
+
+        step = C.c_int32()
+        ptrs = [b.ctypes.data_as(C.POINTER(C.c_double)) for b in self.bufs]
+        while self.s.pending() > 0:
+            for f in range(self.s.n_field):
+                gfb._check(self.s.lib.gfb_read_record(self.s.h, f, C.byref(step), *ptrs, 0))
+            self.count += 1
+
+    def run(self):
+        while not self.halt.is_set():
+            self._read_all()
+            time.sleep(0.0005)
+        self._read_all()
+
+    def stop(self):
+        self.halt.set()
+        self.join()
 
 
 def run_reference(args):
@@ -267,11 +332,14 @@ def run_gfb(args):
     barrier()
     s.synchronize()
     launches0 = s.info()["kernel_launches"]
+    consumer = RecordConsumer(s)
     with ClockSampler(device) as clk:
+        consumer.start()
         t0 = time.perf_counter()
         ms_elem, ms_node, ms_rec = s.advance_profiled(args.steps)
         s.synchronize()
         t1 = time.perf_counter()
+        consumer.stop()
     barrier()
     launches = s.info()["kernel_launches"] - launches0
     wall = t1 - t0
@@ -304,7 +372,7 @@ def run_gfb(args):
     peak, peak_kind = measured_peak_hbm()
     eb = elem_bytes_per_step(prob, info, len(dirs), prec)
     achieved = eb / (ms_elem / args.steps / 1e3) / 1e9
-    nb = node_bytes_per_step(prob, len(dirs), prec)
+    nb = node_bytes_per_step(prob, info, len(dirs), prec)
     traffic = committed_traffic()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -114,9 +115,8 @@ struct DevBuf {
 
 struct Snapshot {
     int step;
-    int slot;            // device ring slot, or -1 once staged on the host
-    cudaEvent_t done;
-    std::vector<double> host;  // staged copy [NFLD][n_rec][NN][15]
+    int slot;                  // ring slot (device + pinned host), -1 once spilled
+    std::vector<double> host;  // spilled copy [NFLD][n_rec][NN][15]
     int fields_read = 0;
     std::vector<char> read_mask;
 };
@@ -133,6 +133,7 @@ struct gfb_solver {
     double dt = 0.0;
     int stride = 0;
     int dirs[3] = {0, 1, 2};
+    int flags = 0;
     int step = 0;
     std::vector<int> colour_begin;  // [n_colour+1] device cell ranges
     std::vector<double> stf;
@@ -154,9 +155,21 @@ struct gfb_solver {
     int *src_head = nullptr, *src_next = nullptr;
     void* src_w = nullptr;
     int* rec_cell = nullptr;
-    double* ring = nullptr;
+    double* ring = nullptr;            // device snapshot ring [slots]
+    std::vector<double*> pinned;       // pinned host copy of each slot
+    std::vector<cudaEvent_t> rec_evt;  // record kernel of the slot done
+    std::vector<cudaEvent_t> copy_evt; // device->host copy of the slot done
+    std::vector<char> copy_issued;
+    int next_slot = 0;
+    // pending snapshots and slot ownership are shared between gfb_advance
+    // and gfb_read_record, which may run on different host threads
+    std::mutex rec_mu;
     std::deque<Snapshot> pending;
-    std::vector<int> free_slots;
+    // C-PML kept at global nodes (FP32 path)
+    bool node_pml = false;
+    int n_pml_node = 0;
+    int* npml_slot = nullptr;
+    void *npml_coef = nullptr, *npml_mem = nullptr, *npml_prev = nullptr;
     long long device_bytes = 0, upload_bytes = 0, launches = 0;
 
     template <typename T>
@@ -173,8 +186,9 @@ struct gfb_solver {
         return GFB_OK;
     }
     ~gfb_solver() {
-        for (auto& s : pending)
-            if (s.done) cudaEventDestroy(s.done);
+        for (auto e : rec_evt) cudaEventDestroy(e);
+        for (auto e : copy_evt) cudaEventDestroy(e);
+        for (auto p : pinned) cudaFreeHost(p);
         bufs.clear();
         if (stream) cudaStreamDestroy(stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
@@ -182,6 +196,23 @@ struct gfb_solver {
 };
 
 namespace {
+
+// Host<->device copies ordered on the solver's stream and complete on return
+// (a plain cudaMemcpy from pageable memory may return before the data has
+// reached the device, and the solver's non-blocking stream does not order
+// against the legacy default stream).
+gfb_status h2d(gfb_solver* s, void* dst, const void* src, size_t bytes) {
+    CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->upload_bytes += (long long)bytes;
+    return GFB_OK;
+}
+
+gfb_status d2h(gfb_solver* s, void* dst, const void* src, size_t bytes) {
+    CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return GFB_OK;
+}
 
 template <typename Real>
 gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
@@ -201,7 +232,7 @@ gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
 
 template <typename Real, int NG, int NFLD>
 gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
-    using S = gfb::Shape<NG>;
+    using S = gfb::FieldShape<NG, NFLD>;
     gfb::ElemArgs<Real> A;
     A.e_begin = s->colour_begin[c];
     A.e_end = s->colour_begin[c + 1];
@@ -211,7 +242,7 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     A.ut = static_cast<const Real*>(s->ut);
     A.force = static_cast<Real*>(s->force);
     A.dmat = static_cast<const Real*>(s->dmat);
-    A.pml_slot = s->has_cpml ? s->pml_slot : nullptr;
+    A.pml_slot = (s->has_cpml && !s->node_pml) ? s->pml_slot : nullptr;
     A.pml_coef = static_cast<const Real*>(s->pml_coef);
     A.pml_mem = static_cast<Real*>(s->pml_mem);
     A.pml_prev = static_cast<Real*>(s->pml_prev);
@@ -229,8 +260,8 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     A.dir2 = s->dirs[2];
     const int n = A.e_end - A.e_begin;
     const int blocks = (n + S::EPB - 1) / S::EPB;
-    const size_t smem = gfb::elem_smem_bytes<Real, NG, NFLD>();
-    gfb::elem_step_kernel<Real, NG, NFLD><<<blocks, S::THREADS, smem, s->stream>>>(A);
+    const size_t smem = gfb::field_smem_bytes<Real, NG, NFLD>();
+    gfb::elem_field_kernel<Real, NG, NFLD><<<blocks, S::THREADS, smem, s->stream>>>(A);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -238,8 +269,8 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
 
 template <typename Real, int NG, int NFLD>
 gfb_status set_smem_t() {
-    const size_t smem = gfb::elem_smem_bytes<Real, NG, NFLD>();
-    CU(cudaFuncSetAttribute(gfb::elem_step_kernel<Real, NG, NFLD>,
+    const size_t smem = gfb::field_smem_bytes<Real, NG, NFLD>();
+    CU(cudaFuncSetAttribute(gfb::elem_field_kernel<Real, NG, NFLD>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return GFB_OK;
 }
@@ -321,7 +352,18 @@ gfb_status launch_node_t(gfb_solver* s) {
     A.beta = 0.0;
     A.gamma = 0.5;
     A.half_dt2 = 0.5 * s->dt * s->dt * (1.0 - 2.0 * A.beta);
-    gfb::node_update_kernel<Real><<<grid_for(A.n, 256), 256, 0, s->stream>>>(A);
+    if (s->node_pml) {
+        gfb::NodePml<Real> P;
+        P.slot = s->npml_slot;
+        P.coef = static_cast<const Real*>(s->npml_coef);
+        P.mem = static_cast<Real*>(s->npml_mem);
+        P.prev = static_cast<Real*>(s->npml_prev);
+        P.c1 = s->c1;
+        P.c2 = s->c2;
+        gfb::node_update_pml_kernel<Real><<<grid_for(A.n, 256), 256, 0, s->stream>>>(A, P);
+    } else {
+        gfb::node_update_kernel<Real><<<grid_for(A.n, 256), 256, 0, s->stream>>>(A);
+    }
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -336,7 +378,7 @@ gfb_status launch_predict_t(gfb_solver* s) {
     const long long n = (long long)s->n_node * s->F;
     const double h = 0.5 * s->dt * s->dt * (1.0 - 2.0 * 0.0);
     gfb::predict_kernel<Real><<<grid_for(n, 256), 256, 0, s->stream>>>(
-        n, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h);
+        n, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -348,24 +390,87 @@ gfb_status launch_predict(gfb_solver* s) {
 
 size_t snapshot_doubles(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
 
-// Move the oldest device-resident snapshot to host memory, freeing its slot.
-gfb_status stage_oldest(gfb_solver* s) {
-    for (auto& snap : s->pending) {
-        if (snap.slot < 0) continue;
-        CU(cudaEventSynchronize(snap.done));
-        snap.host.resize(snapshot_doubles(s));
-        CU(cudaMemcpy(snap.host.data(), s->ring + (size_t)snap.slot * snapshot_doubles(s),
-                      snap.host.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        s->free_slots.push_back(snap.slot);
-        snap.slot = -1;
-        return GFB_OK;
-    }
-    return fail(GFB_ERR_STATE, "no device snapshot to stage");
+// Copy a snapshot out of its pinned slot into pageable memory so the slot can
+// take a new snapshot (only when the caller has not read it yet).
+gfb_status spill(gfb_solver* s, Snapshot& snap) {
+    CU(cudaEventSynchronize(s->copy_evt[snap.slot]));
+    const double* src = s->pinned[snap.slot];
+    snap.host.assign(src, src + snapshot_doubles(s));
+    snap.slot = -1;
+    return GFB_OK;
 }
 
 // ---------------------------------------------------------------------------
 // solver construction
 // ---------------------------------------------------------------------------
+
+// C-PML at global nodes: B_k = sum over C-PML cells at the node of
+// w J/rho A_k (k = 1..5, accumulated in FP64 in cell order), and for each
+// axis the convolution coefficients of the cells where that axis acts.
+// Leaves s->node_pml false (per-cell form) if two cells disagree on an
+// axis's coefficients at a shared node.
+template <typename Real>
+gfb_status build_node_pml(gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w) {
+    const int ng = s->ng, nn = s->nn;
+    std::vector<int> slot(s->n_node, -1);
+    std::vector<double> acc;
+    std::vector<unsigned char> have;
+    int n = 0;
+    for (long long e = 0; e < s->n_cell; ++e) {
+        if (m->pml_region[e] == 0) continue;
+        for (int p = 0; p < nn; ++p) {
+            const long long q = e * nn + p;
+            const double* A = m->pml_coef_abar + q * 5;
+            if (A[0] == 0.0 && A[1] == 0.0 && A[2] == 0.0 && A[3] == 0.0 && A[4] == 0.0) continue;
+            const int g = m->ibool[q];
+            if (slot[g] < 0) {
+                slot[g] = n++;
+                acc.resize((size_t)n * 14, 0.0);
+                have.push_back(0);
+            }
+            double* c = &acc[(size_t)slot[g] * 14];
+            const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
+            const double wgll = w[ni] * w[nj] * w[nk];
+            const double rho = m->density[q];
+            const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
+            for (int k = 0; k < 5; ++k) c[k] += scale * A[k];
+            const double* al = m->pml_coef_alpha + q * 9;
+            for (int ax = 0; ax < 3; ++ax) {
+                if (A[2 + ax] == 0.0) continue;
+                unsigned char& hv = have[slot[g]];
+                if (!(hv & (1u << ax))) {
+                    for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
+                    hv |= (unsigned char)(1u << ax);
+                } else {
+                    for (int t = 0; t < 3; ++t) {
+                        const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
+                        if (std::abs(a0 - a1) > 1e-9 * std::max(std::abs(a0), std::abs(a1))) return GFB_OK;
+                    }
+                }
+            }
+        }
+    }
+    gfb_status st;
+    {
+        int* d = nullptr;
+        if ((st = s->alloc(&d, slot.size()))) return st;
+        if ((st = h2d(s, d, slot.data(), slot.size() * 4))) return st;
+        s->npml_slot = d;
+    }
+    std::vector<Real> coef(acc.size());
+    for (size_t i = 0; i < acc.size(); ++i) coef[i] = (Real)acc[i];
+    if ((st = upload(s, &s->npml_coef, coef))) return st;
+    Real *mem = nullptr, *prev = nullptr;
+    if ((st = s->alloc(&mem, (size_t)n * s->F * 3))) return st;
+    if ((st = s->alloc(&prev, (size_t)n * s->F))) return st;
+    CU(cudaMemset(mem, 0, (size_t)std::max(n, 1) * s->F * 3 * sizeof(Real)));
+    CU(cudaMemset(prev, 0, (size_t)std::max(n, 1) * s->F * sizeof(Real)));
+    s->npml_mem = mem;
+    s->npml_prev = prev;
+    s->n_pml_node = n;
+    s->node_pml = true;
+    return GFB_OK;
+}
 
 template <typename Real>
 gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
@@ -380,8 +485,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     {
         uint32_t* d = nullptr;
         if ((st = s->alloc(&d, ibool_dev.size()))) return st;
-        CU(cudaMemcpy(d, ibool_dev.data(), ibool_dev.size() * 4, cudaMemcpyHostToDevice));
-        s->upload_bytes += (long long)ibool_dev.size() * 4;
+        if ((st = h2d(s, d, ibool_dev.data(), ibool_dev.size() * 4))) return st;
         s->ibool = d;
     }
     // geometry [cell][12][NN] in colour order
@@ -410,27 +514,27 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         if ((st = upload(s, &s->dmat, d))) return st;
     }
     const long long nF = (long long)s->n_node * s->F;
+    const long long nP = (long long)s->n_node * s->nfld * 4;  // [node][field][4]
     if ((st = s->alloc(&s->u, nF))) return st;
     if ((st = s->alloc(&s->v, nF))) return st;
     Real* a = nullptr;
     Real* ut = nullptr;
     Real* force = nullptr;
     if ((st = s->alloc(&a, nF))) return st;
-    if ((st = s->alloc(&ut, nF))) return st;
-    if ((st = s->alloc(&force, nF))) return st;
+    if ((st = s->alloc(&ut, nP))) return st;
+    if ((st = s->alloc(&force, nP))) return st;
     s->a = a;
     s->ut = ut;
     s->force = force;
     CU(cudaMemset(s->u, 0, nF * sizeof(double)));
     CU(cudaMemset(s->v, 0, nF * sizeof(double)));
     CU(cudaMemset(a, 0, nF * sizeof(Real)));
-    CU(cudaMemset(ut, 0, nF * sizeof(Real)));
-    CU(cudaMemset(force, 0, nF * sizeof(Real)));
+    CU(cudaMemset(ut, 0, nP * sizeof(Real)));
+    CU(cudaMemset(force, 0, nP * sizeof(Real)));
     {
         double* d = nullptr;
         if ((st = s->alloc(&d, node_mass.size()))) return st;
-        CU(cudaMemcpy(d, node_mass.data(), node_mass.size() * 8, cudaMemcpyHostToDevice));
-        s->upload_bytes += (long long)node_mass.size() * 8;
+        if ((st = h2d(s, d, node_mass.data(), node_mass.size() * 8))) return st;
         s->mass = d;
     }
     if (s->prec == GFB_FP32) {
@@ -441,11 +545,15 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     if (s->has_damping) {
         double* d = nullptr;
         if ((st = s->alloc(&d, node_damp.size()))) return st;
-        CU(cudaMemcpy(d, node_damp.data(), node_damp.size() * 8, cudaMemcpyHostToDevice));
+        if ((st = h2d(s, d, node_damp.data(), node_damp.size() * 8))) return st;
         s->damping = d;
     }
-    // C-PML cells
-    if (s->has_cpml) {
+    // C-PML at global nodes (FP32 path) when the cells agree at shared nodes
+    if (s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML)) {
+        if ((st = build_node_pml<Real>(s, m, w))) return st;
+    }
+    // C-PML per cell
+    if (s->has_cpml && !s->node_pml) {
         std::vector<int> slot(n_cell, -1);
         std::vector<long long> slot_cell;
         for (long long ed = 0; ed < n_cell; ++ed)
@@ -457,7 +565,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         {
             int* d = nullptr;
             if ((st = s->alloc(&d, slot.size()))) return st;
-            CU(cudaMemcpy(d, slot.data(), slot.size() * 4, cudaMemcpyHostToDevice));
+            if ((st = h2d(s, d, slot.data(), slot.size() * 4))) return st;
             s->pml_slot = d;
         }
         std::vector<Real> coef((size_t)s->n_pml * 15 * nn);
@@ -513,12 +621,16 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         int *dh = nullptr, *dn = nullptr;
         if ((st = s->alloc(&dh, head.size()))) return st;
         if ((st = s->alloc(&dn, next.size()))) return st;
-        CU(cudaMemcpy(dh, head.data(), head.size() * 4, cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(dn, next.data(), next.size() * 4, cudaMemcpyHostToDevice));
+        if ((st = h2d(s, dh, head.data(), head.size() * 4))) return st;
+        if ((st = h2d(s, dn, next.data(), next.size() * 4))) return st;
         s->src_head = dh;
         s->src_next = dn;
         if ((st = upload(s, &s->src_w, wts))) return st;
         s->stf.assign(src->stf, src->stf + std::max(0, src->n_stf));
+    }
+    if (s->node_pml) {
+        s->n_pml = 0;
+        for (long long e = 0; e < n_cell; ++e) s->n_pml += m->pml_region[e] != 0;
     }
     // recording cells and snapshot ring
     if (s->n_rec > 0) {
@@ -526,10 +638,18 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         for (int ci = 0; ci < s->n_rec; ++ci) rc[ci] = inv_perm[m->rec_cell_local[ci]];
         int* d = nullptr;
         if ((st = s->alloc(&d, rc.size()))) return st;
-        CU(cudaMemcpy(d, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice));
+        if ((st = h2d(s, d, rc.data(), rc.size() * 4))) return st;
         s->rec_cell = d;
         if ((st = s->alloc(&s->ring, snapshot_doubles(s) * s->slots))) return st;
-        for (int k = s->slots - 1; k >= 0; --k) s->free_slots.push_back(k);
+        s->pinned.assign(s->slots, nullptr);
+        s->rec_evt.assign(s->slots, nullptr);
+        s->copy_evt.assign(s->slots, nullptr);
+        s->copy_issued.assign(s->slots, 0);
+        for (int k = 0; k < s->slots; ++k) {
+            CU(cudaHostAlloc((void**)&s->pinned[k], snapshot_doubles(s) * sizeof(double), cudaHostAllocDefault));
+            CU(cudaEventCreateWithFlags(&s->rec_evt[k], cudaEventDisableTiming));
+            CU(cudaEventCreateWithFlags(&s->copy_evt[k], cudaEventDisableTiming));
+        }
     }
     return GFB_OK;
 }
@@ -575,16 +695,28 @@ gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
     if ((st = launch_node(s))) return st;
     if (ev) CU(cudaEventRecord(ev[2], s->stream));
     if (s->stride > 0 && s->n_rec > 0 && step % s->stride == 0) {
-        if (s->free_slots.empty())
-            if ((st = stage_oldest(s))) return st;
-        const int slot = s->free_slots.back();
-        s->free_slots.pop_back();
-        if ((st = launch_record(s, s->ring + (size_t)slot * snapshot_doubles(s)))) return st;
+        // round-robin slot; an unread snapshot still in it moves to pageable
+        // memory first.  The record kernel waits (on the GPU) for the last
+        // device->host copy out of the slot; the copy of this snapshot runs
+        // on the copy stream, overlapped with the following steps.
+        std::unique_lock<std::mutex> lk(s->rec_mu);
+        const int slot = s->next_slot;
+        s->next_slot = (s->next_slot + 1) % s->slots;
+        for (auto& old : s->pending)
+            if (old.slot == slot)
+                if ((st = spill(s, old))) return st;
+        if (s->copy_issued[slot]) CU(cudaStreamWaitEvent(s->stream, s->copy_evt[slot], 0));
+        double* dslot = s->ring + (size_t)slot * snapshot_doubles(s);
+        if ((st = launch_record(s, dslot))) return st;
+        CU(cudaEventRecord(s->rec_evt[slot], s->stream));
+        CU(cudaStreamWaitEvent(s->copy_stream, s->rec_evt[slot], 0));
+        CU(cudaMemcpyAsync(s->pinned[slot], dslot, snapshot_doubles(s) * sizeof(double), cudaMemcpyDeviceToHost,
+                           s->copy_stream));
+        CU(cudaEventRecord(s->copy_evt[slot], s->copy_stream));
+        s->copy_issued[slot] = 1;
         Snapshot snap;
         snap.step = step;
         snap.slot = slot;
-        CU(cudaEventCreateWithFlags(&snap.done, cudaEventDisableTiming));
-        CU(cudaEventRecord(snap.done, s->stream));
         snap.read_mask.assign(s->nfld, 0);
         s->pending.push_back(std::move(snap));
     }
@@ -629,6 +761,7 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     s->stride = c->snapshot_stride;
     for (int d = 0; d < 3; ++d) s->dirs[d] = d < c->n_field ? c->field_dir[d] : 0;
     s->has_cpml = m->pml_coef_abar != nullptr;
+    s->flags = c->flags;
     s->n_rec = m->n_rec_cell;
     s->slots = std::max(1, c->record_slots);
     const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
@@ -744,23 +877,31 @@ gfb_status gfb_advance_profiled(gfb_solver* s, int32_t n_steps, double* ms_eleme
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (n_steps < 0) return fail(GFB_ERR_INVALID, "n_steps must be >= 0");
     CU(cudaSetDevice(s->device));
-    cudaEvent_t ev[4];
-    for (auto& e : ev) CU(cudaEventCreate(&e));
-    double acc[3] = {0, 0, 0};
+    std::vector<cudaEvent_t> ev((size_t)n_steps * 4, nullptr);
     gfb_status st = GFB_OK;
-    for (int it = 0; it < n_steps && !st; ++it) {
-        st = one_step(s, ev);
-        if (st) break;
-        CU(cudaEventSynchronize(ev[3]));
-        float t;
-        CU(cudaEventElapsedTime(&t, ev[0], ev[1]));
-        acc[0] += t;
-        CU(cudaEventElapsedTime(&t, ev[1], ev[2]));
-        acc[1] += t;
-        CU(cudaEventElapsedTime(&t, ev[2], ev[3]));
-        acc[2] += t;
+    for (auto& e : ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            st = fail(GFB_ERR_CUDA, "cudaEventCreate failed");
+            break;
+        }
     }
-    for (auto& e : ev) cudaEventDestroy(e);
+    for (int it = 0; it < n_steps && !st; ++it) st = one_step(s, ev.data() + (size_t)it * 4);
+    double acc[3] = {0, 0, 0};
+    if (!st && n_steps > 0) {
+        if (cudaEventSynchronize(ev.back()) != cudaSuccess) st = fail(GFB_ERR_CUDA, "event synchronize failed");
+        for (int it = 0; it < n_steps && !st; ++it) {
+            for (int k = 0; k < 3; ++k) {
+                float t = 0.0f;
+                if (cudaEventElapsedTime(&t, ev[(size_t)it * 4 + k], ev[(size_t)it * 4 + k + 1]) != cudaSuccess) {
+                    st = fail(GFB_ERR_CUDA, "cudaEventElapsedTime failed");
+                    break;
+                }
+                acc[k] += t;
+            }
+        }
+    }
+    for (auto e : ev)
+        if (e) cudaEventDestroy(e);
     if (st) return st;
     if (ms_element) *ms_element += acc[0];
     if (ms_node) *ms_node += acc[1];
@@ -781,6 +922,8 @@ gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
     info->device_bytes = s->device_bytes;
     info->upload_bytes = s->upload_bytes;
     info->kernel_launches = s->launches;
+    info->n_pml_node = s->node_pml ? s->n_pml_node : 0;
+    info->reserved = 0;
     return GFB_OK;
 }
 
@@ -804,24 +947,25 @@ gfb_status gfb_get_state(gfb_solver* s, int32_t field, double* u, double* v, dou
     CU(cudaStreamSynchronize(s->stream));
     const size_t nF = (size_t)s->n_node * s->F;
     std::vector<double> tmp(nF);
+    gfb_status st;
     auto pick = [&](double* dst) {
         for (long long g = 0; g < s->n_node; ++g)
             for (int c = 0; c < 3; ++c) dst[g * 3 + c] = tmp[g * s->F + field * 3 + c];
     };
     if (u) {
-        CU(cudaMemcpy(tmp.data(), s->u, nF * 8, cudaMemcpyDeviceToHost));
+        if ((st = d2h(s, tmp.data(), s->u, nF * 8))) return st;
         pick(u);
     }
     if (v) {
-        CU(cudaMemcpy(tmp.data(), s->v, nF * 8, cudaMemcpyDeviceToHost));
+        if ((st = d2h(s, tmp.data(), s->v, nF * 8))) return st;
         pick(v);
     }
     if (a) {
         if (s->prec == GFB_FP64) {
-            CU(cudaMemcpy(tmp.data(), s->a, nF * 8, cudaMemcpyDeviceToHost));
+            if ((st = d2h(s, tmp.data(), s->a, nF * 8))) return st;
         } else {
             std::vector<float> f(nF);
-            CU(cudaMemcpy(f.data(), s->a, nF * 4, cudaMemcpyDeviceToHost));
+            if ((st = d2h(s, f.data(), s->a, nF * 4))) return st;
             for (size_t i = 0; i < nF; ++i) tmp[i] = f[i];
         }
         pick(a);
@@ -839,17 +983,18 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
     const size_t nF = (size_t)s->n_node * s->F;
     std::vector<double> tmp(nF);
     auto put = [&](const double* src, void* dev, bool is_real_float) -> gfb_status {
+        gfb_status st;
         if (is_real_float) {
             std::vector<float> f(nF);
-            CU(cudaMemcpy(f.data(), dev, nF * 4, cudaMemcpyDeviceToHost));
+            if ((st = d2h(s, f.data(), dev, nF * 4))) return st;
             for (long long g = 0; g < s->n_node; ++g)
                 for (int c = 0; c < 3; ++c) f[g * s->F + field * 3 + c] = src ? (float)src[g * 3 + c] : 0.0f;
-            CU(cudaMemcpy(dev, f.data(), nF * 4, cudaMemcpyHostToDevice));
+            if ((st = h2d(s, dev, f.data(), nF * 4))) return st;
         } else {
-            CU(cudaMemcpy(tmp.data(), dev, nF * 8, cudaMemcpyDeviceToHost));
+            if ((st = d2h(s, tmp.data(), dev, nF * 8))) return st;
             for (long long g = 0; g < s->n_node; ++g)
                 for (int c = 0; c < 3; ++c) tmp[g * s->F + field * 3 + c] = src ? src[g * 3 + c] : 0.0;
-            CU(cudaMemcpy(dev, tmp.data(), nF * 8, cudaMemcpyHostToDevice));
+            if ((st = h2d(s, dev, tmp.data(), nF * 8))) return st;
         }
         return GFB_OK;
     };
@@ -857,10 +1002,14 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
     if ((st = put(u, s->u, false))) return st;
     if ((st = put(v, s->v, false))) return st;
     if ((st = put(a, s->a, s->prec == GFB_FP32))) return st;
-    if (s->has_cpml) {
+    if (s->has_cpml && !s->node_pml) {
         const size_t es = s->prec == GFB_FP64 ? 8 : 4;
         CU(cudaMemset(s->pml_mem, 0, (size_t)s->n_pml * s->F * 3 * s->nn * es));
         CU(cudaMemset(s->pml_prev, 0, (size_t)s->n_pml * s->F * s->nn * es));
+    }
+    if (s->node_pml && s->n_pml_node > 0) {
+        CU(cudaMemset(s->npml_mem, 0, (size_t)s->n_pml_node * s->F * 3 * sizeof(float)));
+        CU(cudaMemset(s->npml_prev, 0, (size_t)s->n_pml_node * s->F * sizeof(float)));
     }
     if ((st = launch_predict(s))) return st;
     CU(cudaStreamSynchronize(s->stream));
@@ -870,6 +1019,7 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
 
 gfb_status gfb_records_pending(gfb_solver* s, int32_t* n) {
     if (!s || !n) return fail(GFB_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->rec_mu);
     *n = (int32_t)s->pending.size();
     return GFB_OK;
 }
@@ -878,18 +1028,15 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
                            double* v, double* a, int32_t release) {
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
-    if (s->pending.empty()) return fail(GFB_ERR_STATE, "no snapshot pending");
     CU(cudaSetDevice(s->device));
+    std::lock_guard<std::mutex> lk(s->rec_mu);
+    if (s->pending.empty()) return fail(GFB_ERR_STATE, "no snapshot pending");
     Snapshot& snap = s->pending.front();
     const size_t per_field = (size_t)s->n_rec * s->nn * 15;
-    std::vector<double> buf(per_field);
     const double* src;
     if (snap.slot >= 0) {
-        CU(cudaEventSynchronize(snap.done));
-        CU(cudaMemcpyAsync(buf.data(), s->ring + (size_t)snap.slot * snapshot_doubles(s) + field * per_field,
-                           per_field * 8, cudaMemcpyDeviceToHost, s->copy_stream));
-        CU(cudaStreamSynchronize(s->copy_stream));
-        src = buf.data();
+        CU(cudaEventSynchronize(s->copy_evt[snap.slot]));
+        src = s->pinned[snap.slot] + field * per_field;
     } else {
         src = snap.host.data() + field * per_field;
     }
@@ -909,11 +1056,7 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
         snap.read_mask[field] = 1;
         snap.fields_read++;
     }
-    if (release || snap.fields_read == s->nfld) {
-        if (snap.slot >= 0) s->free_slots.push_back(snap.slot);
-        cudaEventDestroy(snap.done);
-        s->pending.pop_front();
-    }
+    if (release || snap.fields_read == s->nfld) s->pending.pop_front();
     return GFB_OK;
 }
 
@@ -954,22 +1097,31 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
     gfb_status st = gfb_create(&m, &c, nullptr, &s);
     if (st) return st;
     std::unique_ptr<gfb_solver, gfb_status (*)(gfb_solver*)> guard(s, gfb_destroy);
-    const size_t nF = (size_t)P * 3;
+    // [point][4] padded vectors on the device
+    const size_t nP = (size_t)P * 4;
     if (precision == GFB_FP64) {
-        CU(cudaMemcpy(s->ut, u, nF * 8, cudaMemcpyHostToDevice));
+        std::vector<double> h(nP, 0.0);
+        for (long long q = 0; q < P; ++q)
+            for (int c = 0; c < 3; ++c) h[q * 4 + c] = u[q * 3 + c];
+        if ((st = h2d(s, s->ut, h.data(), nP * 8))) return st;
     } else {
-        std::vector<float> f(nF);
-        for (size_t i = 0; i < nF; ++i) f[i] = (float)u[i];
-        CU(cudaMemcpy(s->ut, f.data(), nF * 4, cudaMemcpyHostToDevice));
+        std::vector<float> h(nP, 0.0f);
+        for (long long q = 0; q < P; ++q)
+            for (int c = 0; c < 3; ++c) h[q * 4 + c] = (float)u[q * 3 + c];
+        if ((st = h2d(s, s->ut, h.data(), nP * 4))) return st;
     }
     if ((st = launch_elem(s, 0, 0.0))) return st;
     CU(cudaStreamSynchronize(s->stream));
     if (precision == GFB_FP64) {
-        CU(cudaMemcpy(r, s->force, nF * 8, cudaMemcpyDeviceToHost));
+        std::vector<double> h(nP);
+        if ((st = d2h(s, h.data(), s->force, nP * 8))) return st;
+        for (long long q = 0; q < P; ++q)
+            for (int c = 0; c < 3; ++c) r[q * 3 + c] = h[q * 4 + c];
     } else {
-        std::vector<float> f(nF);
-        CU(cudaMemcpy(f.data(), s->force, nF * 4, cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < nF; ++i) r[i] = f[i];
+        std::vector<float> h(nP);
+        if ((st = d2h(s, h.data(), s->force, nP * 4))) return st;
+        for (long long q = 0; q < P; ++q)
+            for (int c = 0; c < 3; ++c) r[q * 3 + c] = h[q * 4 + c];
     }
     return GFB_OK;
 }

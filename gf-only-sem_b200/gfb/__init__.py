@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libgfb.so")
 HEADER_PATH = os.path.join(os.path.dirname(PKG_ROOT), "include", "gfb.h")
 
 FP64, FP32 = 0, 1
+FLAG_CELL_PML = 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -66,6 +67,7 @@ class Config(C.Structure):
         ("field_dir", C.c_int32 * 3),
         ("device", C.c_int32),
         ("record_slots", C.c_int32),
+        ("flags", C.c_int32),
     ]
 
 
@@ -82,6 +84,8 @@ class Info(C.Structure):
         ("device_bytes", C.c_int64),
         ("upload_bytes", C.c_int64),
         ("kernel_launches", C.c_int64),
+        ("n_pml_node", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -167,7 +171,7 @@ class Solver:
     """
 
     def __init__(self, prob: dict, dirs: Sequence[int] = (0,), precision: int = FP64,
-                 device: int = 0, record_slots: int = 4, record: bool = True):
+                 device: int = 0, record_slots: int = 4, record: bool = True, flags: int = 0):
         self.lib = load_library()
         keep = {}
 
@@ -212,6 +216,7 @@ class Solver:
             c.field_dir[i] = int(d)
         c.device = int(device)
         c.record_slots = int(record_slots)
+        c.flags = int(flags)
         s = Source()
         ids = arr("src_cell_ids", np.int64)
         s.n_src_cell = 0 if ids is None else int(ids.size)

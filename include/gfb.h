@@ -81,7 +81,14 @@ typedef struct gfb_config {
     int32_t field_dir[3];      /* force direction per wavefield, 0=x 1=y 2=z   */
     int32_t device;            /* CUDA device ordinal                          */
     int32_t record_slots;      /* snapshot slots kept on the device (>=1)      */
+    int32_t flags;             /* GFB_FLAG_* bits, 0 for defaults              */
 } gfb_config;
+
+/* Keep C-PML memory per cell and GLL node, as the reference does
+ * (pml.cpp:112-149), also on the FP32 path.  Without it the FP32 path keeps
+ * one memory per global node and axis when the cells' axis coefficients
+ * agree at every shared node (they are functions of the node position). */
+#define GFB_FLAG_CELL_PML 1
 
 /* Point-force source (config.h5 /source, io.cpp:681-707). */
 typedef struct gfb_source {
@@ -125,7 +132,9 @@ gfb_status gfb_destroy(gfb_solver* solver);
  * Replaces cuda_newmark_predict, cuda_gather_predicted, cuda_zero_residual,
  * cuda_launch_element_residual, cuda_pml_damping, cuda_source_injection,
  * cuda_scatter_to_rank and cuda_newmark_correct (cuda_step.hpp:87-117).
- * Returns GFB_ERR_STATE if un-read snapshots would be overwritten.
+ * Snapshots are copied to pinned host memory on a second stream while the
+ * following steps run; when all record_slots hold unread snapshots, the
+ * oldest is moved to ordinary host memory, so none is lost.
  */
 gfb_status gfb_advance(gfb_solver* solver, int32_t n_steps);
 
@@ -152,6 +161,8 @@ typedef struct gfb_info {
     int64_t device_bytes;    /* device memory held                                         */
     int64_t upload_bytes;    /* bytes copied host->device by gfb_create                    */
     int64_t kernel_launches; /* kernels launched by this solver so far                     */
+    int32_t n_pml_node;      /* global nodes carrying C-PML state (0: per-cell form)        */
+    int32_t reserved;
 } gfb_info;
 
 gfb_status gfb_get_info(const gfb_solver* solver, gfb_info* info);
@@ -177,7 +188,10 @@ gfb_status gfb_get_state(gfb_solver* solver, int32_t field, double* u, double* v
 gfb_status gfb_set_state(gfb_solver* solver, int32_t field, int32_t step, const double* u,
                          const double* v, const double* a);
 
-/* Number of snapshots waiting to be read. */
+/* Number of snapshots waiting to be read.  gfb_records_pending and
+ * gfb_read_record may be called from another host thread while
+ * gfb_advance runs (a writer thread draining records); all other calls on a
+ * solver must come from one thread at a time. */
 gfb_status gfb_records_pending(gfb_solver* solver, int32_t* n);
 
 /*

@@ -50,6 +50,17 @@ def test_element_kernel_fp64_matches_oracle(ngll):
     assert rel < 1e-12, rel
 
 
+@pytest.mark.parametrize("n_elem,prec", [(262, gfb.FP64), (300, gfb.FP64), (600, gfb.FP32), (2000, gfb.FP32)])
+def test_element_kernel_sizes_around_the_host_copy_staging(n_elem, prec):
+    """Inputs of about 1 MB, where a pageable-memory copy used to return
+    before reaching the device and the kernel read a stale tail."""
+    dxi, jac, lam, mu, u = random_elements(5, n_elem, 11)
+    ref = oracle.element_residual(dxi, jac, lam, mu, u, 5)
+    got = gfb.element_residual(dxi, jac, lam, mu, u, 5, prec)
+    tol = 1e-12 if prec == gfb.FP64 else 1e-5
+    assert np.abs(got - ref).max() / np.abs(ref).max() < tol
+
+
 @pytest.mark.parametrize("ngll", [4, 5])
 def test_element_kernel_fp32_and_rigid_translation(ngll):
     dxi, jac, lam, mu, u = random_elements(ngll, 5, 7)
@@ -124,6 +135,46 @@ def test_fp32_batched_within_1e4_of_fp64_oracle():
     for d in range(3):
         ref, _ = oracle_snaps(prob, d, n)
         compare_runs(snaps[d], ref, FP32_TOL, f"fp32 field {d}")
+
+
+def test_fp32_node_and_cell_cpml_forms_agree():
+    """The FP32 path keeps C-PML memory per global node when the cells agree
+    on each axis's coefficients at shared nodes; the per-cell form
+    (GFB_FLAG_CELL_PML, the reference's pml.cpp:112-216 layout) must give the
+    same traces to FP32 rounding, and both stay within 1e-4 of the oracle."""
+    prob = layered_problem(nsteps=200)
+    n = prob["nsteps"]
+    node = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32)
+    cell = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, flags=gfb.FLAG_CELL_PML)
+    assert node.info()["n_pml_node"] > 0 and cell.info()["n_pml_node"] == 0
+    node.advance(n)
+    cell.advance(n)
+    a, b = node.drain(), cell.drain()
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(a[d], ref, FP32_TOL, f"node-cpml field {d}")
+        for k in ("u", "strain"):
+            assert rel_l2(a[d][k], b[d][k]) < 1e-5
+
+
+def test_node_cpml_falls_back_when_cell_coefficients_disagree():
+    prob = layered_problem(nsteps=40)
+    nc = prob["n_cell"]
+    alpha = prob["pml_coef_alpha"].copy().reshape(nc, -1, 9)
+    A3 = prob["pml_coef_abar"].reshape(nc, -1, 5)[:, :, 2]
+    ib = prob["ibool"].reshape(nc, -1)
+    # a cell whose x-axis memory term (A3) is live at a node it shares with
+    # another cell where it is live too; perturb that cell's x coefficients
+    live = np.zeros(prob["n_node"], dtype=int)
+    np.add.at(live, ib[A3 != 0], 1)
+    e = next(c for c in range(nc) if np.any(live[ib[c][A3[c] != 0]] > 1))
+    alpha[e, :, 1] *= 1.01
+    prob["pml_coef_alpha"] = alpha
+    s = gfb.Solver(prob, dirs=[0], precision=gfb.FP32)
+    assert s.info()["n_pml_node"] == 0
+    s.advance(40)
+    ref, _ = oracle_snaps(prob, 0, 40)
+    compare_runs(s.drain()[0], ref, FP32_TOL, "fallback")
 
 
 @pytest.mark.parametrize("prec", [gfb.FP64, gfb.FP32])
