@@ -23,7 +23,8 @@
 // Layouts on the device (cells in colour order):
 //   ibool  [cell][NN]            node id | FIRST_TOUCH bit
 //   geom   [cell][12][NN] Real   dxi_dx(9), jac*w_i*w_j*w_k, lambda, mu
-//   state  [node][F]             F = 3 * n_field; u, v in double, a/ut/force in Real
+//   state  u, v (double), a (Real): [node][3*n_field];
+//          predicted displacement ut and force (Real): [node][n_field][4]
 //   C-PML  coef [slot][15][NN] Real (alpha 9, abar 5, w*J/rho),
 //          mem [slot][n_field*9][NN], prev [slot][n_field*3][NN]
 #pragma once
@@ -64,9 +65,10 @@ struct ElemArgs {
     const Real* pml_coef;  // [slot][15][NN]
     Real* pml_mem;         // [slot][F*3][NN]
     Real* pml_prev;        // [slot][F][NN]
-    const double* u;
+    const double* u;     // [node][3*n_field]
     const double* v;
     const Real* a;
+    long long n_node;
     double c1, c2;
     // source
     const int* src_head;  // [cell] first source slot or -1
@@ -250,37 +252,7 @@ constexpr size_t elem_smem_bytes() {
     return sizeof(Real) * (64 + (size_t)S::EPB * 3 * NFLD * S::NNP * 4);
 }
 
-// ---------------------------------------------------------------------------
-// elem_field_kernel: the time loop's element/assembly kernel.
-//
-// One thread per (GLL point, wavefield): the three wavefields of a point run
-// in three different warps, so a thread holds one field's gradient and
-// stress and there are three times more warps to cover the gather latency
-// than with one thread per point.  Per cell:
-//   1. the cell's geometry block [12][NN] (contiguous, 16-byte multiple) is
-//      staged into shared memory with 16-byte loads by all the cell's
-//      threads; each thread gathers its node's field as one 16-byte vector
-//      ([node][field][4] layout) into shared memory;
-//   2. gradient from 3 x NG neighbour vectors, Hooke stress in registers;
-//   3. for each reference axis: the flux jw * sigma . (dd[a], dd[3+a],
-//      dd[6+a]) goes to the same shared buffer, and the divergence
-//      contribution is summed from NG neighbour vectors of that axis;
-//   4. C-PML per-cell term (FP64 path / per-cell form), point force, and
-//      the colour-ordered read-modify-write of the node's force vector.
-// Shared memory per cell: 12*NN + 4*NN*n_field words.
-// ---------------------------------------------------------------------------
-
-template <int NG, int NFLD>
-struct FieldShape {
-    static constexpr int NN = NG * NG * NG;
-    static constexpr int NNP = (NN + 31) / 32 * 32;
-    static constexpr int TPE = NNP * NFLD;                  // threads per cell
-    static constexpr int EPB = TPE >= 256 ? 1 : 256 / TPE;  // cells per block
-    static constexpr int THREADS = TPE * EPB;
-    static constexpr int GEO = 12 * NN;                     // geometry words per cell
-    static constexpr int BUF = 4 * NN * NFLD;               // vector words per cell
-};
-
+// 16-byte vector helpers (a float4, or two double2 for FP64 vectors).
 __device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
     const float4 t = *reinterpret_cast<const float4*>(p);
     v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
@@ -305,220 +277,316 @@ __device__ __forceinline__ void store4(double* p, double a, double b, double c, 
     reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
 }
 
-template <typename Real, int NG, int NFLD>
-constexpr size_t field_smem_bytes() {
-    using S = FieldShape<NG, NFLD>;
-    return sizeof(Real) * (64 + (size_t)S::EPB * (S::GEO + S::BUF));
+// ---------------------------------------------------------------------------
+// elem_pipe_kernel: persistent, software-pipelined element/assembly kernel.
+//
+// Blocks loop over groups of EPB cells of one colour.  While group i is
+// computed, the gathered displacement of group i+1 and the geometry + node
+// table of group i+2 are in flight as cp.async copies into rotating shared
+// stages (3 stages for geometry/ibool, 2 for the gathered vectors), so each
+// SM keeps tens of KB of loads outstanding independent of how many blocks
+// fit.  Thread per GLL point; the n_field wavefields are looped per thread.
+// Node table on the device is padded to NNP entries per cell so every copy
+// is a 16-byte cp.async.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <typename Real, int NG, int NFLD>
-__global__ void __launch_bounds__(FieldShape<NG, NFLD>::THREADS) elem_field_kernel(ElemArgs<Real> A) {
-    using S = FieldShape<NG, NFLD>;
-    constexpr int NN = S::NN, NNP = S::NNP, TPE = S::TPE, EPB = S::EPB, F = 3 * NFLD;
-    static_assert((S::GEO * sizeof(Real)) % 16 == 0, "geometry block must be a 16-byte multiple");
+struct PipeShape {
+    static constexpr int NN = NG * NG * NG;
+    static constexpr int NNP = (NN + 31) / 32 * 32;
+    static constexpr int EPB = NNP <= 32 ? 8 : (NNP <= 64 ? 4 : (NNP <= 128 ? 2 : 1));
+    static constexpr int THREADS = NNP * EPB;
+    static constexpr int GEO_B = 12 * NN * (int)sizeof(Real);         // geometry bytes per cell
+    static constexpr int IB_B = NNP * 4;                               // node-table bytes per cell
+    static constexpr int BUF_B = NN * NFLD * 4 * (int)sizeof(Real);    // field vectors per cell
+    // a geometry stage also receives the cell's old force vectors once the
+    // geometry has been read into registers
+    static constexpr int GEO_SLOT = GEO_B > BUF_B ? GEO_B : BUF_B;
+    static constexpr int GSTAGE = EPB * GEO_SLOT;
+    static constexpr int ISTAGE = EPB * IB_B;
+    static constexpr int BSTAGE = EPB * BUF_B;
+    static constexpr int D_B = 64 * (int)sizeof(Real);
+    static constexpr int SMEM = D_B + 2 * GSTAGE + 3 * ISTAGE + 2 * BSTAGE;
+    static constexpr int MIN_BLOCKS = (64 * 1024) / (THREADS * 64) > 0 ? (64 * 1024) / (THREADS * 64) : 1;
+    static_assert(GEO_B % 16 == 0 && IB_B % 16 == 0 && BUF_B % 16 == 0, "16-byte copies");
+};
+
+template <typename Real, int NG, int NFLD>
+__global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Real) == 4 ? PipeShape<Real, NG, NFLD>::MIN_BLOCKS : 1))
+    elem_pipe_kernel(ElemArgs<Real> A, const uint32_t* __restrict__ ibool_padded, int n_groups) {
+    using S = PipeShape<Real, NG, NFLD>;
+    constexpr int NN = S::NN, NNP = S::NNP, EPB = S::EPB, THREADS = S::THREADS;
+    constexpr int VW = 16 / (int)sizeof(Real);               // Reals per 16-byte copy
+    constexpr int CPV = 4 * (int)sizeof(Real) / 16;          // 16-byte copies per field vector
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real* sD = reinterpret_cast<Real*>(smem_raw);
+    unsigned char* gbase = smem_raw + S::D_B;
+    unsigned char* ibase = gbase + 2 * S::GSTAGE;
+    unsigned char* bbase = ibase + 3 * S::ISTAGE;
     const int tid = threadIdx.x;
-    const int el = tid / TPE;
-    const int rem = tid - el * TPE;
-    const int d = rem / NNP;
-    const int p = rem - d * NNP;
-    const int e = A.e_begin + blockIdx.x * EPB + el;
-    const bool cell_ok = e < A.e_end;
-    const bool active = cell_ok && p < NN;
-    Real* geo = sD + 64 + el * (S::GEO + S::BUF);
-    Real* buf = geo + S::GEO;
+    const int el = tid / NNP, p = tid - el * NNP;
     if (tid < NG * NG) sD[tid] = A.dmat[tid];
-    if (cell_ok) {
-        constexpr int CH = (int)(S::GEO * sizeof(Real) / 16);
-        const uint4* src = reinterpret_cast<const uint4*>(A.geom + (size_t)e * S::GEO);
-        uint4* dst = reinterpret_cast<uint4*>(geo);
-        for (int q = rem; q < CH; q += TPE) dst[q] = __ldg(src + q);
-    }
-    uint32_t gword = 0;
-    if (active) {
-        gword = __ldg(A.ibool + (size_t)e * NN + p);
-        Real v[4];
-        load4_nc(A.ut + ((size_t)(gword & kNodeMask) * NFLD + d) * 4, v);
-        store4(buf + (p * NFLD + d) * 4, v[0], v[1], v[2], v[3]);
-    }
+
+    auto geo_of = [&](int st, int c) -> Real* {
+        return reinterpret_cast<Real*>(gbase + st * S::GSTAGE + c * S::GEO_SLOT);
+    };
+    auto ib_of = [&](int st, int c) -> uint32_t* {
+        return reinterpret_cast<uint32_t*>(ibase + st * S::ISTAGE + c * S::IB_B);
+    };
+    auto buf_of = [&](int st, int c) -> Real* {
+        return reinterpret_cast<Real*>(bbase + st * S::BSTAGE + c * S::BUF_B);
+    };
+    auto issue_ib = [&](int grp, int st) {
+        constexpr int CI = S::IB_B / 16;
+        for (int q = tid; q < EPB * CI; q += THREADS) {
+            const int c = q / CI, r = q - c * CI;
+            const int e = A.e_begin + grp * EPB + c;
+            if (e < A.e_end)
+                cp_async16(reinterpret_cast<unsigned char*>(ib_of(st, c)) + r * 16,
+                           reinterpret_cast<const unsigned char*>(ibool_padded) + (size_t)e * S::IB_B + r * 16);
+        }
+    };
+    auto issue_geo = [&](int grp, int st) {
+        constexpr int CG = S::GEO_B / 16;
+        for (int q = tid; q < EPB * CG; q += THREADS) {
+            const int c = q / CG, r = q - c * CG;
+            const int e = A.e_begin + grp * EPB + c;
+            if (e < A.e_end)
+                cp_async16(reinterpret_cast<unsigned char*>(geo_of(st, c)) + r * 16,
+                           reinterpret_cast<const unsigned char*>(A.geom) + (size_t)e * S::GEO_B + r * 16);
+        }
+    };
+    // this point's predicted-displacement vectors (node table in stage ist)
+    auto issue_gather = [&](int grp, int ist, int bs) {
+        const int e = A.e_begin + grp * EPB + el;
+        if (e >= A.e_end || p >= NN) return;
+        const uint32_t g = ib_of(ist, el)[p] & kNodeMask;
+#pragma unroll
+        for (int d = 0; d < NFLD; ++d)
+#pragma unroll
+            for (int h = 0; h < CPV; ++h)
+                cp_async16(buf_of(bs, el) + (p * NFLD + d) * 4 + h * VW, A.ut + ((size_t)g * NFLD + d) * 4 + h * VW);
+    };
+
+    // prologue: node table of the first group, then its vectors and
+    // geometry and the node table of the second group
+    const int grp0 = blockIdx.x;
+    if (grp0 < n_groups) issue_ib(grp0, 0);
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
+    if (grp0 < n_groups) {
+        issue_gather(grp0, 0, 0);
+        issue_geo(grp0, 0);
+    }
+    if (grp0 + (int)gridDim.x < n_groups) issue_ib(grp0 + gridDim.x, 1);
+    cp_async_commit();
+
     const int i = p / (NG * NG), j = (p / NG) % NG, k = p % NG;
-    Real dd[9], jw = Real(0);
-    Real s00 = 0, s11 = 0, s22 = 0, s01 = 0, s02 = 0, s12 = 0;
-    if (active) {
+    int it = 0;
+    for (int grp = grp0; grp < n_groups; grp += gridDim.x, ++it) {
+        const int cur = it & 1, ist = it % 3;
+        cp_async_wait_all();
+        __syncthreads();  // vectors + geometry of this group, node table of the next
+        const int e = A.e_begin + grp * EPB + el;
+        const bool active = (e < A.e_end) && (p < NN);
+        Real* geo = geo_of(cur, el);
+        Real* buf = buf_of(cur, el);
+        uint32_t gword = 0;
+        Real dd[9], jw = Real(0), lam = Real(0), mu = Real(0);
+        if (active) {
+            gword = ib_of(ist, el)[p];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) dd[q] = geo[q * NN + p];
-        jw = geo[9 * NN + p];
-        const Real lam = geo[10 * NN + p], mu = geo[11 * NN + p];
-        if (mu > Real(0)) {  // element_cpu.cpp:42-43: mu <= 0 adds nothing
-            Real gx[3] = {0, 0, 0}, gy[3] = {0, 0, 0}, gz[3] = {0, 0, 0};
+            for (int q = 0; q < 9; ++q) dd[q] = geo[q * NN + p];
+            jw = geo[9 * NN + p];
+            lam = geo[10 * NN + p];
+            mu = geo[11 * NN + p];
+        }
+        __syncthreads();  // geometry stage now takes this group's old force vectors
+        if (active && !(gword & kFirstTouch)) {
+            const uint32_t g = gword & kNodeMask;
 #pragma unroll
-            for (int s = 0; s < NG; ++s) {
-                Real va[4], vb[4], vc[4];
-                load4(buf + ((((s * NG + j) * NG + k) * NFLD) + d) * 4, va);
-                load4(buf + ((((i * NG + s) * NG + k) * NFLD) + d) * 4, vb);
-                load4(buf + ((((i * NG + j) * NG + s) * NFLD) + d) * 4, vc);
-                const Real Di = sD[i * NG + s], Dj = sD[j * NG + s], Dk = sD[k * NG + s];
+            for (int d = 0; d < NFLD; ++d)
+#pragma unroll
+                for (int h = 0; h < CPV; ++h)
+                    cp_async16(geo + (p * NFLD + d) * 4 + h * VW, A.force + ((size_t)g * NFLD + d) * 4 + h * VW);
+        }
+        cp_async_commit();  // group: old force of this group
+        const int nxt = grp + gridDim.x;
+        if (nxt < n_groups) {
+            issue_gather(nxt, (it + 1) % 3, cur ^ 1);
+            issue_geo(nxt, cur ^ 1);
+        }
+        if (nxt + (int)gridDim.x < n_groups) issue_ib(nxt + gridDim.x, (it + 2) % 3);
+        cp_async_commit();  // group: next group's vectors and geometry, node table after that
+
+        Real st[NFLD][6];
+#pragma unroll
+        for (int d = 0; d < NFLD; ++d)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) st[d][q] = Real(0);
+        if (active && mu > Real(0)) {  // element_cpu.cpp:42-43: mu <= 0 adds nothing
+#pragma unroll
+            for (int d = 0; d < NFLD; ++d) {
+                Real gx[3] = {0, 0, 0}, gy[3] = {0, 0, 0}, gz[3] = {0, 0, 0};
+#pragma unroll
+                for (int s = 0; s < NG; ++s) {
+                    Real va[4], vb[4], vc[4];
+                    load4(buf + ((((s * NG + j) * NG + k) * NFLD) + d) * 4, va);
+                    load4(buf + ((((i * NG + s) * NG + k) * NFLD) + d) * 4, vb);
+                    load4(buf + ((((i * NG + j) * NG + s) * NFLD) + d) * 4, vc);
+                    const Real Di = sD[i * NG + s], Dj = sD[j * NG + s], Dk = sD[k * NG + s];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        gx[c] += Di * va[c];
+                        gy[c] += Dj * vb[c];
+                        gz[c] += Dk * vc[c];
+                    }
+                }
+                Real gr[3][3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    gx[c] += Di * va[c];
-                    gy[c] += Dj * vb[c];
-                    gz[c] += Dk * vc[c];
+                    gr[c][0] = gx[c] * dd[0] + gy[c] * dd[1] + gz[c] * dd[2];
+                    gr[c][1] = gx[c] * dd[3] + gy[c] * dd[4] + gz[c] * dd[5];
+                    gr[c][2] = gx[c] * dd[6] + gy[c] * dd[7] + gz[c] * dd[8];
+                }
+                const Real tr = gr[0][0] + gr[1][1] + gr[2][2];
+                const Real m2 = Real(2) * mu;
+                st[d][0] = m2 * gr[0][0] + lam * tr;
+                st[d][1] = m2 * gr[1][1] + lam * tr;
+                st[d][2] = m2 * gr[2][2] + lam * tr;
+                st[d][3] = m2 * (Real(0.5) * (gr[0][1] + gr[1][0]));
+                st[d][4] = m2 * (Real(0.5) * (gr[0][2] + gr[2][0]));
+                st[d][5] = m2 * (Real(0.5) * (gr[1][2] + gr[2][1]));
+            }
+        }
+        __syncthreads();  // the vector buffer is reused for the fluxes
+        Real r[NFLD][3];
+#pragma unroll
+        for (int d = 0; d < NFLD; ++d) r[d][0] = r[d][1] = r[d][2] = Real(0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (active) {
+                const Real ea = dd[a], eb = dd[3 + a], ec = dd[6 + a];
+#pragma unroll
+                for (int d = 0; d < NFLD; ++d)
+                    store4(buf + (p * NFLD + d) * 4, jw * (st[d][0] * ea + st[d][3] * eb + st[d][4] * ec),
+                           jw * (st[d][3] * ea + st[d][1] * eb + st[d][5] * ec),
+                           jw * (st[d][4] * ea + st[d][5] * eb + st[d][2] * ec), Real(0));
+            }
+            __syncthreads();
+            if (active) {
+                const int ia = (a == 0) ? i : ((a == 1) ? j : k);
+#pragma unroll
+                for (int s = 0; s < NG; ++s) {
+                    const int q = (a == 0) ? ((s * NG + j) * NG + k)
+                                           : ((a == 1) ? ((i * NG + s) * NG + k) : ((i * NG + j) * NG + s));
+                    const Real w = sD[s * NG + ia];
+#pragma unroll
+                    for (int d = 0; d < NFLD; ++d) {
+                        Real v[4];
+                        load4(buf + (q * NFLD + d) * 4, v);
+                        r[d][0] -= w * v[0];
+                        r[d][1] -= w * v[1];
+                        r[d][2] -= w * v[2];
+                    }
                 }
             }
-            Real gr[3][3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                gr[c][0] = gx[c] * dd[0] + gy[c] * dd[1] + gz[c] * dd[2];
-                gr[c][1] = gx[c] * dd[3] + gy[c] * dd[4] + gz[c] * dd[5];
-                gr[c][2] = gx[c] * dd[6] + gy[c] * dd[7] + gz[c] * dd[8];
-            }
-            const Real tr = gr[0][0] + gr[1][1] + gr[2][2];
-            const Real m2 = Real(2) * mu;
-            s00 = m2 * gr[0][0] + lam * tr;
-            s11 = m2 * gr[1][1] + lam * tr;
-            s22 = m2 * gr[2][2] + lam * tr;
-            s01 = m2 * (Real(0.5) * (gr[0][1] + gr[1][0]));
-            s02 = m2 * (Real(0.5) * (gr[0][2] + gr[2][0]));
-            s12 = m2 * (Real(0.5) * (gr[1][2] + gr[2][1]));
+            if (a < 2) __syncthreads();
         }
-    }
-    __syncthreads();  // buf is reused for the fluxes
-    Real r0 = Real(0), r1 = Real(0), r2 = Real(0);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
         if (active) {
-            const Real ea = dd[a], eb = dd[3 + a], ec = dd[6 + a];
-            store4(buf + (p * NFLD + d) * 4, jw * (s00 * ea + s01 * eb + s02 * ec),
-                   jw * (s01 * ea + s11 * eb + s12 * ec), jw * (s02 * ea + s12 * eb + s22 * ec), Real(0));
+            const uint32_t g = gword & kNodeMask;
+            // C-PML per cell (pml.cpp:55-216)
+            const int slot = A.pml_slot ? __ldg(A.pml_slot + e) : -1;
+            if (slot >= 0) {
+                const Real* cf = A.pml_coef + (size_t)slot * 15 * NN + p;
+                Real al[9], ab[5];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) al[q] = __ldg(cf + q * NN);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) ab[q] = __ldg(cf + (9 + q) * NN);
+                const Real scale = __ldg(cf + 14 * NN);
+                Real* mem = A.pml_mem + (size_t)slot * (3 * NFLD * 3) * NN + p;
+                Real* prev = A.pml_prev + (size_t)slot * (3 * NFLD) * NN + p;
+#pragma unroll
+                for (int d = 0; d < NFLD; ++d) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int f = d * 3 + c;
+                        const double un = A.u[(size_t)g * 3 * NFLD + f];
+                        const double vn = A.v[(size_t)g * 3 * NFLD + f];
+                        const Real an = A.a[(size_t)g * 3 * NFLD + f];
+                        const Real nv = Real(un + A.c1 * vn);
+                        const Real ov = prev[f * NN] + Real(A.c2) * an;
+                        Real m0 = mem[(f * 3 + 0) * NN], m1 = mem[(f * 3 + 1) * NN], m2 = mem[(f * 3 + 2) * NN];
+                        r[d][c] += scale * (ab[0] * Real(vn) + ab[1] * Real(un) + ab[2] * m0 + ab[3] * m1 + ab[4] * m2);
+                        mem[(f * 3 + 0) * NN] = al[0] * m0 + al[1] * nv + al[2] * ov;
+                        mem[(f * 3 + 1) * NN] = al[3] * m1 + al[4] * nv + al[5] * ov;
+                        mem[(f * 3 + 2) * NN] = al[6] * m2 + al[7] * nv + al[8] * ov;
+                        prev[f * NN] = nv;
+                    }
+                }
+            }
+            // point force (solver.cpp:577-605)
+            if (A.stf != Real(0)) {
+                int s = A.src_head ? __ldg(A.src_head + e) : -1;
+                while (s >= 0) {
+                    const Real w = __ldg(A.src_w + (size_t)s * NN + p);
+                    if (w != Real(0)) {
+                        const Real sw = A.stf * w;
+#pragma unroll
+                        for (int d = 0; d < NFLD; ++d) {
+                            const int dir = (d == 0) ? A.dir0 : ((d == 1) ? A.dir1 : A.dir2);
+#pragma unroll
+                            for (int c = 0; c < 3; ++c)
+                                if (c == dir) r[d][c] += sw;
+                        }
+                    }
+                    s = __ldg(A.src_next + s);
+                }
+            }
         }
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this group's old force
         __syncthreads();
         if (active) {
-            const int ia = (a == 0) ? i : ((a == 1) ? j : k);
+            const uint32_t g = gword & kNodeMask;
+            const bool first = gword & kFirstTouch;
 #pragma unroll
-            for (int s = 0; s < NG; ++s) {
-                const int q = (a == 0) ? ((s * NG + j) * NG + k) : ((a == 1) ? ((i * NG + s) * NG + k) : ((i * NG + j) * NG + s));
-                Real v[4];
-                load4(buf + (q * NFLD + d) * 4, v);
-                const Real w = sD[s * NG + ia];
-                r0 -= w * v[0];
-                r1 -= w * v[1];
-                r2 -= w * v[2];
+            for (int d = 0; d < NFLD; ++d) {
+                Real* out = A.force + ((size_t)g * NFLD + d) * 4;
+                if (first) {
+                    store4(out, r[d][0], r[d][1], r[d][2], Real(0));
+                } else {
+                    Real fo[4];
+                    load4(geo + (p * NFLD + d) * 4, fo);
+                    store4(out, fo[0] + r[d][0], fo[1] + r[d][1], fo[2] + r[d][2], Real(0));
+                }
             }
         }
-        if (a < 2) __syncthreads();
     }
-    if (!active) return;
-    const uint32_t g = gword & kNodeMask;
-    // C-PML per cell (pml.cpp:55-216), as in elem_step_kernel
-    const int slot = A.pml_slot ? __ldg(A.pml_slot + e) : -1;
-    if (slot >= 0) {
-        const Real* cf = A.pml_coef + (size_t)slot * 15 * NN + p;
-        Real al[9], ab[5];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) al[q] = __ldg(cf + q * NN);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) ab[q] = __ldg(cf + (9 + q) * NN);
-        const Real scale = __ldg(cf + 14 * NN);
-        Real* mem = A.pml_mem + (size_t)slot * (F * 3) * NN + p;
-        Real* prev = A.pml_prev + (size_t)slot * F * NN + p;
-        Real rr[3] = {r0, r1, r2};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const int f = d * 3 + c;
-            const double un = A.u[(size_t)g * F + f];
-            const double vn = A.v[(size_t)g * F + f];
-            const Real an = A.a[(size_t)g * F + f];
-            const Real nv = Real(un + A.c1 * vn);
-            const Real ov = prev[f * NN] + Real(A.c2) * an;
-            Real m0 = mem[(f * 3 + 0) * NN], m1 = mem[(f * 3 + 1) * NN], m2 = mem[(f * 3 + 2) * NN];
-            rr[c] += scale * (ab[0] * Real(vn) + ab[1] * Real(un) + ab[2] * m0 + ab[3] * m1 + ab[4] * m2);
-            m0 = al[0] * m0 + al[1] * nv + al[2] * ov;
-            m1 = al[3] * m1 + al[4] * nv + al[5] * ov;
-            m2 = al[6] * m2 + al[7] * nv + al[8] * ov;
-            mem[(f * 3 + 0) * NN] = m0;
-            mem[(f * 3 + 1) * NN] = m1;
-            mem[(f * 3 + 2) * NN] = m2;
-            prev[f * NN] = nv;
-        }
-        r0 = rr[0];
-        r1 = rr[1];
-        r2 = rr[2];
-    }
-    // point force (solver.cpp:577-605)
-    if (A.stf != Real(0)) {
-        const int dir = (d == 0) ? A.dir0 : ((d == 1) ? A.dir1 : A.dir2);
-        int s = A.src_head ? __ldg(A.src_head + e) : -1;
-        while (s >= 0) {
-            const Real w = __ldg(A.src_w + (size_t)s * NN + p);
-            if (w != Real(0)) {
-                const Real sw = A.stf * w;
-                if (dir == 0) r0 += sw;
-                else if (dir == 1) r1 += sw;
-                else r2 += sw;
-            }
-            s = __ldg(A.src_next + s);
-        }
-    }
-    Real* out = A.force + ((size_t)g * NFLD + d) * 4;
-    if (gword & kFirstTouch) {
-        store4(out, r0, r1, r2, Real(0));
-    } else {
-        Real v[4];
-        load4(out, v);
-        store4(out, v[0] + r0, v[1] + r1, v[2] + r2, Real(0));
-    }
+    cp_async_wait_all();
 }
 
 template <typename Real>
 struct NodeArgs {
-    long long n;      // n_node * F
-    int F;
-    double* u;
+    long long n_node;
+    double* u;              // [node][3*n_field]
     double* v;
     Real* a;
-    Real* ut;
-    const Real* force;
+    Real* ut;               // [node][field][4]
+    const Real* force;      // [node][field][4]
     const double* mass;     // [n_node] assembled lumped mass
     const Real* inv_mass;   // [n_node] 1/m (FP32 path) or nullptr
     const double* damping;  // [n_node] or nullptr
     double dt, half_dt2, beta, gamma;
 };
-
-// Newmark corrector (solver.cpp:52-69, with the legacy damping of 564-574
-// applied to v first) followed by the next step's predictor (40-49).
-template <typename Real>
-__global__ void node_update_kernel(NodeArgs<Real> A) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < A.n; idx += stride) {
-        const long long g = idx / A.F;
-        const int f = (int)(idx - g * A.F);
-        const long long pi = padded_index(g, f, A.F);
-        double vv = A.v[idx];
-        if (A.damping) {
-            const double d = A.damping[g];
-            if (d > 0.0) vv -= d * vv;
-        }
-        double uu = A.u[idx];
-        const double m = A.mass[g];
-        double a_new;
-        if (m <= 0.0) {
-            a_new = 0.0;
-        } else {
-            const double a_old = (double)A.a[idx];
-            if (A.inv_mass) a_new = (double)(A.force[pi] * A.inv_mass[g]);
-            else a_new = (double)A.force[pi] / m;
-            a_new = (double)(Real)a_new;
-            uu += A.dt * vv + A.dt * A.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
-            vv += A.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
-        }
-        A.u[idx] = uu;
-        A.v[idx] = vv;
-        A.a[idx] = (Real)a_new;
-        A.ut[pi] = (Real)(uu + A.dt * vv + A.half_dt2 * a_new);
-    }
-}
 
 // C-PML at global nodes (FP32 path).
 //
@@ -542,77 +610,100 @@ struct NodePml {
     double c1, c2;
 };
 
-template <typename Real>
-__global__ void node_update_pml_kernel(NodeArgs<Real> A, NodePml<Real> P) {
+// One thread per (node, wavefield), the wavefields of a node in adjacent
+// threads, so a warp streams contiguous u, v, a and force/prediction
+// vectors and reads each node's mass / C-PML slot once: node C-PML term
+// (when P.slot), Newmark corrector (solver.cpp:52-69, legacy damping of
+// 564-574 applied to v first) and the next step's predictor (40-49).
+template <typename Real, int NFLD, bool PML>
+__global__ void node_update_kernel(NodeArgs<Real> A, NodePml<Real> P) {
+    constexpr int F = 3 * NFLD;
+    const long long total = A.n_node * NFLD;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < A.n; idx += stride) {
-        const long long g = idx / A.F;
-        const int f = (int)(idx - g * A.F);
-        const long long pi = padded_index(g, f, A.F);
-        double vv = A.v[idx];
-        double uu = A.u[idx];
-        const double a_old = (double)A.a[idx];
-        Real force = A.force[pi];
-        const int sl = __ldg(P.slot + g);
-        if (sl >= 0) {
-            const Real* cf = P.coef + (size_t)sl * 14;
-            Real* m = P.mem + ((size_t)sl * A.F + f) * 3;
-            Real* pv = P.prev + (size_t)sl * A.F + f;
-            const Real nv = (Real)(uu + P.c1 * vv);
-            const Real ov = *pv + (Real)P.c2 * (Real)a_old;
-            const Real m0 = m[0], m1 = m[1], m2 = m[2];
-            force += __ldg(cf + 0) * (Real)vv + __ldg(cf + 1) * (Real)uu + __ldg(cf + 2) * m0 +
-                     __ldg(cf + 3) * m1 + __ldg(cf + 4) * m2;
-            if (__ldg(cf + 2) != Real(0)) m[0] = __ldg(cf + 5) * m0 + __ldg(cf + 6) * nv + __ldg(cf + 7) * ov;
-            if (__ldg(cf + 3) != Real(0)) m[1] = __ldg(cf + 8) * m1 + __ldg(cf + 9) * nv + __ldg(cf + 10) * ov;
-            if (__ldg(cf + 4) != Real(0)) m[2] = __ldg(cf + 11) * m2 + __ldg(cf + 12) * nv + __ldg(cf + 13) * ov;
-            *pv = nv;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const long long g = t / NFLD;
+        const int d = (int)(t - g * NFLD);
+        const double m = A.mass[g];
+        const double dmp = A.damping ? A.damping[g] : 0.0;
+        const Real im = A.inv_mass ? A.inv_mass[g] : Real(0);
+        Real fv[4];
+        load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv);
+        int sl = -1;
+        if (PML) sl = __ldg(P.slot + g);
+        Real out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int f = d * 3 + c;
+            const long long idx = g * F + f;
+            double vv = A.v[idx];
+            if (dmp > 0.0) vv -= dmp * vv;
+            double uu = A.u[idx];
+            const double a_old = (double)A.a[idx];
+            Real force = fv[c];
+            if (PML && sl >= 0) {
+                const Real* cf = P.coef + (size_t)sl * 14;
+                Real* mm = P.mem + ((size_t)sl * F + f) * 3;
+                Real* pv = P.prev + (size_t)sl * F + f;
+                const Real nv = (Real)(uu + P.c1 * vv);
+                const Real ov = *pv + (Real)P.c2 * (Real)a_old;
+                const Real m0 = mm[0], m1 = mm[1], m2 = mm[2];
+                force += cf[0] * (Real)vv + cf[1] * (Real)uu + cf[2] * m0 + cf[3] * m1 + cf[4] * m2;
+                if (cf[2] != Real(0)) mm[0] = cf[5] * m0 + cf[6] * nv + cf[7] * ov;
+                if (cf[3] != Real(0)) mm[1] = cf[8] * m1 + cf[9] * nv + cf[10] * ov;
+                if (cf[4] != Real(0)) mm[2] = cf[11] * m2 + cf[12] * nv + cf[13] * ov;
+                *pv = nv;
+            }
+            double a_new;
+            if (m <= 0.0) {
+                a_new = 0.0;
+            } else {
+                a_new = A.inv_mass ? (double)(force * im) : (double)force / m;
+                a_new = (double)(Real)a_new;
+                uu += A.dt * vv + A.dt * A.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
+                vv += A.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
+            }
+            A.u[idx] = uu;
+            A.v[idx] = vv;
+            A.a[idx] = (Real)a_new;
+            out[c] = (Real)(uu + A.dt * vv + A.half_dt2 * a_new);
         }
-        const double mass = A.mass[g];
-        double a_new;
-        if (mass <= 0.0) {
-            a_new = 0.0;
-        } else {
-            a_new = (double)(Real)(force * A.inv_mass[g]);
-            uu += A.dt * vv + A.dt * A.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
-            vv += A.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
-        }
-        A.u[idx] = uu;
-        A.v[idx] = vv;
-        A.a[idx] = (Real)a_new;
-        A.ut[pi] = (Real)(uu + A.dt * vv + A.half_dt2 * a_new);
+        store4(A.ut + ((size_t)g * NFLD + d) * 4, out[0], out[1], out[2], Real(0));
     }
 }
 
 // Predictor only (start of a run or after a state overwrite).
 template <typename Real>
-__global__ void predict_kernel(long long n, int F, const double* u, const double* v, const Real* a,
+__global__ void predict_kernel(long long n_node, int F, const double* u, const double* v, const Real* a,
                                Real* ut, double dt, double half_dt2) {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
+    const long long total = n_node * F;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
         const long long g = idx / F;
-        ut[padded_index(g, (int)(idx - g * F), F)] = (Real)(u[idx] + dt * v[idx] + half_dt2 * (double)a[idx]);
+        const int f = (int)(idx - g * F);
+        ut[padded_index(g, f, F)] = (Real)(u[idx] + dt * v[idx] + half_dt2 * (double)a[idx]);
+        if (f % 3 == 2) ut[padded_index(g, f, F) + 1] = Real(0);
     }
 }
 
-template <typename Real>
+template <typename Real, typename Out>
 struct RecArgs {
     int n_rec;
     const int* rec_cell;    // [n_rec] device cell index
     const uint32_t* ibool;
     const Real* geom;
     const Real* dmat;
-    const double* u;
+    const double* u;        // [node][3*n_field]
     const double* v;
     const Real* a;
-    double* out;            // [NFLD][n_rec][NN][15]
+    long long n_node;
+    Out* out;               // [NFLD][n_rec][NN][15]
 };
 
 // Snapshot of the recording cells: strain from the gathered corrected
 // displacement (solver.cpp:282-335) plus u, v, a at every cell node
 // (solver.cpp:485-504).  One block per recording cell.
-template <typename Real, int NG, int NFLD>
-__global__ void record_kernel(RecArgs<Real> A) {
+template <typename Real, int NG, int NFLD, typename Out>
+__global__ void record_kernel(RecArgs<Real, Out> A) {
     using S = Shape<NG>;
     constexpr int NN = S::NN, F = 3 * NFLD;
     __shared__ double su[F][NN];
@@ -648,17 +739,17 @@ __global__ void record_kernel(RecArgs<Real> A) {
             gr[c][1] = gx[c] * dd[3] + gy[c] * dd[4] + gz[c] * dd[5];
             gr[c][2] = gx[c] * dd[6] + gy[c] * dd[7] + gz[c] * dd[8];
         }
-        double* o = A.out + (((size_t)d * A.n_rec + ci) * NN + p) * 15;
-        o[0] = gr[0][0];
-        o[1] = gr[1][1];
-        o[2] = gr[2][2];
-        o[3] = 0.5 * (gr[0][1] + gr[1][0]);
-        o[4] = 0.5 * (gr[0][2] + gr[2][0]);
-        o[5] = 0.5 * (gr[1][2] + gr[2][1]);
+        Out* o = A.out + (((size_t)d * A.n_rec + ci) * NN + p) * 15;
+        o[0] = (Out)gr[0][0];
+        o[1] = (Out)gr[1][1];
+        o[2] = (Out)gr[2][2];
+        o[3] = (Out)(0.5 * (gr[0][1] + gr[1][0]));
+        o[4] = (Out)(0.5 * (gr[0][2] + gr[2][0]));
+        o[5] = (Out)(0.5 * (gr[1][2] + gr[2][1]));
         for (int c = 0; c < 3; ++c) {
-            o[6 + c] = A.u[(size_t)g * F + d * 3 + c];
-            o[9 + c] = A.v[(size_t)g * F + d * 3 + c];
-            o[12 + c] = (double)A.a[(size_t)g * F + d * 3 + c];
+            o[6 + c] = (Out)A.u[(size_t)g * F + d * 3 + c];
+            o[9 + c] = (Out)A.v[(size_t)g * F + d * 3 + c];
+            o[12 + c] = (Out)A.a[(size_t)g * F + d * 3 + c];
         }
     }
 }

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <condition_variable>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -118,6 +119,7 @@ struct Snapshot {
     int slot;                  // ring slot (device + pinned host), -1 once spilled
     std::vector<double> host;  // spilled copy [NFLD][n_rec][NN][15]
     int fields_read = 0;
+    int readers = 0;           // gfb_read_record calls copying out of the slot
     std::vector<char> read_mask;
 };
 
@@ -143,6 +145,8 @@ struct gfb_solver {
     // device memory
     std::vector<std::unique_ptr<DevBuf>> bufs;
     uint32_t* ibool = nullptr;
+    uint32_t* ibool_padded = nullptr;  // [cell][NNP] for the pipelined kernel
+    int pipe_blocks = 0;               // persistent grid of the element kernel
     void* geom = nullptr;
     void* dmat = nullptr;
     double *u = nullptr, *v = nullptr;
@@ -155,8 +159,9 @@ struct gfb_solver {
     int *src_head = nullptr, *src_next = nullptr;
     void* src_w = nullptr;
     int* rec_cell = nullptr;
-    double* ring = nullptr;            // device snapshot ring [slots]
-    std::vector<double*> pinned;       // pinned host copy of each slot
+    void* ring = nullptr;              // device snapshot ring [slots]
+    std::vector<void*> pinned;         // pinned host copy of each slot
+    bool rec_f32 = false;              // snapshot values stored as float
     std::vector<cudaEvent_t> rec_evt;  // record kernel of the slot done
     std::vector<cudaEvent_t> copy_evt; // device->host copy of the slot done
     std::vector<char> copy_issued;
@@ -164,6 +169,7 @@ struct gfb_solver {
     // pending snapshots and slot ownership are shared between gfb_advance
     // and gfb_read_record, which may run on different host threads
     std::mutex rec_mu;
+    std::condition_variable rec_cv;
     std::deque<Snapshot> pending;
     // C-PML kept at global nodes (FP32 path)
     bool node_pml = false;
@@ -232,7 +238,7 @@ gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
 
 template <typename Real, int NG, int NFLD>
 gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
-    using S = gfb::FieldShape<NG, NFLD>;
+    using S = gfb::PipeShape<Real, NG, NFLD>;
     gfb::ElemArgs<Real> A;
     A.e_begin = s->colour_begin[c];
     A.e_end = s->colour_begin[c + 1];
@@ -249,6 +255,7 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     A.u = s->u;
     A.v = s->v;
     A.a = static_cast<const Real*>(s->a);
+    A.n_node = s->n_node;
     A.c1 = s->c1;
     A.c2 = s->c2;
     A.src_head = s->has_src ? s->src_head : nullptr;
@@ -259,26 +266,32 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     A.dir1 = s->dirs[1];
     A.dir2 = s->dirs[2];
     const int n = A.e_end - A.e_begin;
-    const int blocks = (n + S::EPB - 1) / S::EPB;
-    const size_t smem = gfb::field_smem_bytes<Real, NG, NFLD>();
-    gfb::elem_field_kernel<Real, NG, NFLD><<<blocks, S::THREADS, smem, s->stream>>>(A);
+    const int groups = (n + S::EPB - 1) / S::EPB;
+    const int blocks = std::max(1, std::min(groups, s->pipe_blocks));
+    gfb::elem_pipe_kernel<Real, NG, NFLD><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A, s->ibool_padded, groups);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
 }
 
 template <typename Real, int NG, int NFLD>
-gfb_status set_smem_t() {
-    const size_t smem = gfb::field_smem_bytes<Real, NG, NFLD>();
-    CU(cudaFuncSetAttribute(gfb::elem_field_kernel<Real, NG, NFLD>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+gfb_status set_smem_t(gfb_solver* s) {
+    using S = gfb::PipeShape<Real, NG, NFLD>;
+    CU(cudaFuncSetAttribute(gfb::elem_pipe_kernel<Real, NG, NFLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            S::SMEM));
+    int per_sm = 0, n_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gfb::elem_pipe_kernel<Real, NG, NFLD>, S::THREADS,
+                                                     S::SMEM));
+    CU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->device));
+    if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "element kernel does not fit on an SM");
+    s->pipe_blocks = per_sm * n_sm;
     return GFB_OK;
 }
 
-template <typename Real, int NG, int NFLD>
-gfb_status launch_record_t(gfb_solver* s, double* out) {
+template <typename Real, int NG, int NFLD, typename Out>
+gfb_status launch_record_o(gfb_solver* s, Out* out) {
     using S = gfb::Shape<NG>;
-    gfb::RecArgs<Real> A;
+    gfb::RecArgs<Real, Out> A;
     A.n_rec = s->n_rec;
     A.rec_cell = s->rec_cell;
     A.ibool = s->ibool;
@@ -287,11 +300,18 @@ gfb_status launch_record_t(gfb_solver* s, double* out) {
     A.u = s->u;
     A.v = s->v;
     A.a = static_cast<const Real*>(s->a);
+    A.n_node = s->n_node;
     A.out = out;
-    gfb::record_kernel<Real, NG, NFLD><<<s->n_rec, S::NNP, 0, s->stream>>>(A);
+    gfb::record_kernel<Real, NG, NFLD, Out><<<s->n_rec, S::NNP, 0, s->stream>>>(A);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
+}
+
+template <typename Real, int NG, int NFLD>
+gfb_status launch_record_t(gfb_solver* s, void* out) {
+    if (s->rec_f32) return launch_record_o<Real, NG, NFLD, float>(s, static_cast<float*>(out));
+    return launch_record_o<Real, NG, NFLD, double>(s, static_cast<double*>(out));
 }
 
 // Instantiate (Real, NG, NFLD) combinations behind one switch.
@@ -313,11 +333,11 @@ struct ElemOp {
 };
 template <typename Real, int NG, int NFLD>
 struct SmemOp {
-    static gfb_status run() { return set_smem_t<Real, NG, NFLD>(); }
+    static gfb_status run(gfb_solver* s) { return set_smem_t<Real, NG, NFLD>(s); }
 };
 template <typename Real, int NG, int NFLD>
 struct RecOp {
-    static gfb_status run(gfb_solver* s, double* out) { return launch_record_t<Real, NG, NFLD>(s, out); }
+    static gfb_status run(gfb_solver* s, void* out) { return launch_record_t<Real, NG, NFLD>(s, out); }
 };
 
 gfb_status launch_elem(gfb_solver* s, int c, double stf) {
@@ -325,7 +345,7 @@ gfb_status launch_elem(gfb_solver* s, int c, double stf) {
     return dispatch<float, ElemOp>(s->ng, s->nfld, s, c, stf);
 }
 
-gfb_status launch_record(gfb_solver* s, double* out) {
+gfb_status launch_record(gfb_solver* s, void* out) {
     if (s->prec == GFB_FP64) return dispatch<double, RecOp>(s->ng, s->nfld, s, out);
     return dispatch<float, RecOp>(s->ng, s->nfld, s, out);
 }
@@ -335,11 +355,10 @@ int grid_for(long long n, int threads) {
     return (int)std::max(1LL, std::min(b, 148LL * 32));
 }
 
-template <typename Real>
-gfb_status launch_node_t(gfb_solver* s) {
+template <typename Real, int NFLD>
+gfb_status launch_node_f(gfb_solver* s) {
     gfb::NodeArgs<Real> A;
-    A.n = (long long)s->n_node * s->F;
-    A.F = s->F;
+    A.n_node = s->n_node;
     A.u = s->u;
     A.v = s->v;
     A.a = static_cast<Real*>(s->a);
@@ -352,21 +371,29 @@ gfb_status launch_node_t(gfb_solver* s) {
     A.beta = 0.0;
     A.gamma = 0.5;
     A.half_dt2 = 0.5 * s->dt * s->dt * (1.0 - 2.0 * A.beta);
+    gfb::NodePml<Real> P{};
+    const int grid = grid_for((long long)s->n_node * NFLD, 256);
     if (s->node_pml) {
-        gfb::NodePml<Real> P;
         P.slot = s->npml_slot;
         P.coef = static_cast<const Real*>(s->npml_coef);
         P.mem = static_cast<Real*>(s->npml_mem);
         P.prev = static_cast<Real*>(s->npml_prev);
         P.c1 = s->c1;
         P.c2 = s->c2;
-        gfb::node_update_pml_kernel<Real><<<grid_for(A.n, 256), 256, 0, s->stream>>>(A, P);
+        gfb::node_update_kernel<Real, NFLD, true><<<grid, 256, 0, s->stream>>>(A, P);
     } else {
-        gfb::node_update_kernel<Real><<<grid_for(A.n, 256), 256, 0, s->stream>>>(A);
+        gfb::node_update_kernel<Real, NFLD, false><<<grid, 256, 0, s->stream>>>(A, P);
     }
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
+}
+
+template <typename Real>
+gfb_status launch_node_t(gfb_solver* s) {
+    if (s->nfld == 1) return launch_node_f<Real, 1>(s);
+    if (s->nfld == 2) return launch_node_f<Real, 2>(s);
+    return launch_node_f<Real, 3>(s);
 }
 
 gfb_status launch_node(gfb_solver* s) {
@@ -378,7 +405,7 @@ gfb_status launch_predict_t(gfb_solver* s) {
     const long long n = (long long)s->n_node * s->F;
     const double h = 0.5 * s->dt * s->dt * (1.0 - 2.0 * 0.0);
     gfb::predict_kernel<Real><<<grid_for(n, 256), 256, 0, s->stream>>>(
-        n, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h);
+        (long long)s->n_node, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -388,14 +415,25 @@ gfb_status launch_predict(gfb_solver* s) {
     return s->prec == GFB_FP64 ? launch_predict_t<double>(s) : launch_predict_t<float>(s);
 }
 
-size_t snapshot_doubles(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
+size_t snapshot_values(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
+size_t snapshot_bytes(const gfb_solver* s) { return snapshot_values(s) * (s->rec_f32 ? 4 : 8); }
+
+// Convert n snapshot values starting at value `off` of a pinned slot to double.
+void slot_values(const gfb_solver* s, int slot, size_t off, size_t n, double* dst) {
+    if (s->rec_f32) {
+        const float* src = static_cast<const float*>(s->pinned[slot]) + off;
+        for (size_t i = 0; i < n; ++i) dst[i] = src[i];
+    } else {
+        std::memcpy(dst, static_cast<const double*>(s->pinned[slot]) + off, n * sizeof(double));
+    }
+}
 
 // Copy a snapshot out of its pinned slot into pageable memory so the slot can
 // take a new snapshot (only when the caller has not read it yet).
 gfb_status spill(gfb_solver* s, Snapshot& snap) {
     CU(cudaEventSynchronize(s->copy_evt[snap.slot]));
-    const double* src = s->pinned[snap.slot];
-    snap.host.assign(src, src + snapshot_doubles(s));
+    snap.host.resize(snapshot_values(s));
+    slot_values(s, snap.slot, 0, snap.host.size(), snap.host.data());
     snap.slot = -1;
     return GFB_OK;
 }
@@ -487,6 +525,14 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         if ((st = s->alloc(&d, ibool_dev.size()))) return st;
         if ((st = h2d(s, d, ibool_dev.data(), ibool_dev.size() * 4))) return st;
         s->ibool = d;
+        const int nnp = (nn + 31) / 32 * 32;
+        std::vector<uint32_t> pad((size_t)n_cell * nnp, 0u);
+        for (long long e = 0; e < n_cell; ++e)
+            for (int p = 0; p < nn; ++p) pad[e * nnp + p] = ibool_dev[e * nn + p];
+        uint32_t* dp = nullptr;
+        if ((st = s->alloc(&dp, pad.size()))) return st;
+        if ((st = h2d(s, dp, pad.data(), pad.size() * 4))) return st;
+        s->ibool_padded = dp;
     }
     // geometry [cell][12][NN] in colour order
     {
@@ -640,13 +686,15 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         if ((st = s->alloc(&d, rc.size()))) return st;
         if ((st = h2d(s, d, rc.data(), rc.size() * 4))) return st;
         s->rec_cell = d;
-        if ((st = s->alloc(&s->ring, snapshot_doubles(s) * s->slots))) return st;
+        unsigned char* ring = nullptr;
+        if ((st = s->alloc(&ring, snapshot_bytes(s) * s->slots))) return st;
+        s->ring = ring;
         s->pinned.assign(s->slots, nullptr);
         s->rec_evt.assign(s->slots, nullptr);
         s->copy_evt.assign(s->slots, nullptr);
         s->copy_issued.assign(s->slots, 0);
         for (int k = 0; k < s->slots; ++k) {
-            CU(cudaHostAlloc((void**)&s->pinned[k], snapshot_doubles(s) * sizeof(double), cudaHostAllocDefault));
+            CU(cudaHostAlloc(&s->pinned[k], snapshot_bytes(s), cudaHostAllocDefault));
             CU(cudaEventCreateWithFlags(&s->rec_evt[k], cudaEventDisableTiming));
             CU(cudaEventCreateWithFlags(&s->copy_evt[k], cudaEventDisableTiming));
         }
@@ -703,15 +751,17 @@ gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
         const int slot = s->next_slot;
         s->next_slot = (s->next_slot + 1) % s->slots;
         for (auto& old : s->pending)
-            if (old.slot == slot)
-                if ((st = spill(s, old))) return st;
+            if (old.slot == slot) {
+                s->rec_cv.wait(lk, [&] { return old.readers == 0; });  // a reader is copying it out
+                if (old.slot == slot)
+                    if ((st = spill(s, old))) return st;
+            }
         if (s->copy_issued[slot]) CU(cudaStreamWaitEvent(s->stream, s->copy_evt[slot], 0));
-        double* dslot = s->ring + (size_t)slot * snapshot_doubles(s);
+        void* dslot = static_cast<unsigned char*>(s->ring) + (size_t)slot * snapshot_bytes(s);
         if ((st = launch_record(s, dslot))) return st;
         CU(cudaEventRecord(s->rec_evt[slot], s->stream));
         CU(cudaStreamWaitEvent(s->copy_stream, s->rec_evt[slot], 0));
-        CU(cudaMemcpyAsync(s->pinned[slot], dslot, snapshot_doubles(s) * sizeof(double), cudaMemcpyDeviceToHost,
-                           s->copy_stream));
+        CU(cudaMemcpyAsync(s->pinned[slot], dslot, snapshot_bytes(s), cudaMemcpyDeviceToHost, s->copy_stream));
         CU(cudaEventRecord(s->copy_evt[slot], s->copy_stream));
         s->copy_issued[slot] = 1;
         Snapshot snap;
@@ -762,6 +812,7 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     for (int d = 0; d < 3; ++d) s->dirs[d] = d < c->n_field ? c->field_dir[d] : 0;
     s->has_cpml = m->pml_coef_abar != nullptr;
     s->flags = c->flags;
+    s->rec_f32 = (c->flags & GFB_FLAG_RECORD_F32) != 0;
     s->n_rec = m->n_rec_cell;
     s->slots = std::max(1, c->record_slots);
     const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
@@ -840,10 +891,10 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     std::vector<double> x, w, D;
     if (!gll_tables(m->ngll - 1, x, w, D)) return fail(GFB_ERR_INVALID, "GLL table construction failed");
     if (s->prec == GFB_FP64) {
-        if ((st = dispatch<double, SmemOp>(s->ng, s->nfld))) return st;
+        if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<double>(s.get(), m, src, perm, inv_perm, ibool_dev, node_mass, node_damp, w, D);
     } else {
-        if ((st = dispatch<float, SmemOp>(s->ng, s->nfld))) return st;
+        if ((st = dispatch<float, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<float>(s.get(), m, src, perm, inv_perm, ibool_dev, node_mass, node_damp, w, D);
     }
     if (st) return st;
@@ -948,7 +999,7 @@ gfb_status gfb_get_state(gfb_solver* s, int32_t field, double* u, double* v, dou
     const size_t nF = (size_t)s->n_node * s->F;
     std::vector<double> tmp(nF);
     gfb_status st;
-    auto pick = [&](double* dst) {
+    auto pick = [&](double* dst) {  // device layout [node][3*n_field]
         for (long long g = 0; g < s->n_node; ++g)
             for (int c = 0; c < 3; ++c) dst[g * 3 + c] = tmp[g * s->F + field * 3 + c];
     };
@@ -1029,35 +1080,58 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
     CU(cudaSetDevice(s->device));
-    std::lock_guard<std::mutex> lk(s->rec_mu);
-    if (s->pending.empty()) return fail(GFB_ERR_STATE, "no snapshot pending");
-    Snapshot& snap = s->pending.front();
     const size_t per_field = (size_t)s->n_rec * s->nn * 15;
-    const double* src;
-    if (snap.slot >= 0) {
-        CU(cudaEventSynchronize(s->copy_evt[snap.slot]));
-        src = s->pinned[snap.slot] + field * per_field;
-    } else {
-        src = snap.host.data() + field * per_field;
+    Snapshot* snap;
+    int slot;
+    {
+        std::lock_guard<std::mutex> lk(s->rec_mu);
+        if (s->pending.empty()) return fail(GFB_ERR_STATE, "no snapshot pending");
+        snap = &s->pending.front();
+        snap->readers++;  // keeps the slot from being spilled or reused while copying
+        slot = snap->slot;
     }
-    if (step) *step = snap.step;
-    const size_t npt = (size_t)s->n_rec * s->nn;
-    for (size_t q = 0; q < npt; ++q) {
-        const double* o = src + q * 15;
-        if (strain)
-            for (int c = 0; c < 6; ++c) strain[q * 6 + c] = o[c];
-        for (int c = 0; c < 3; ++c) {
-            if (u) u[q * 3 + c] = o[6 + c];
-            if (v) v[q * 3 + c] = o[9 + c];
-            if (a) a[q * 3 + c] = o[12 + c];
+    // copy out without holding the lock (the stepping thread may go on)
+    std::vector<double> buf;
+    const double* src = nullptr;
+    const bool want = strain || u || v || a;
+    gfb_status st = GFB_OK;
+    if (slot >= 0) {
+        if (cudaEventSynchronize(s->copy_evt[slot]) != cudaSuccess) st = fail(GFB_ERR_CUDA, "snapshot copy failed");
+        if (want) {
+            buf.resize(per_field);
+            if (!st) slot_values(s, slot, field * per_field, per_field, buf.data());
+            src = buf.data();
+        }
+    } else {
+        src = snap->host.data() + field * per_field;
+    }
+    if (step) *step = snap->step;
+    if (!st && want) {
+        const size_t npt = (size_t)s->n_rec * s->nn;
+        for (size_t q = 0; q < npt; ++q) {
+            const double* o = src + q * 15;
+            if (strain)
+                for (int c = 0; c < 6; ++c) strain[q * 6 + c] = o[c];
+            for (int c = 0; c < 3; ++c) {
+                if (u) u[q * 3 + c] = o[6 + c];
+                if (v) v[q * 3 + c] = o[9 + c];
+                if (a) a[q * 3 + c] = o[12 + c];
+            }
         }
     }
-    if (!snap.read_mask[field]) {
-        snap.read_mask[field] = 1;
-        snap.fields_read++;
+    {
+        std::lock_guard<std::mutex> lk(s->rec_mu);
+        snap->readers--;
+        if (!st) {
+            if (!snap->read_mask[field]) {
+                snap->read_mask[field] = 1;
+                snap->fields_read++;
+            }
+            if (release || snap->fields_read == s->nfld) s->pending.pop_front();
+        }
     }
-    if (release || snap.fields_read == s->nfld) s->pending.pop_front();
-    return GFB_OK;
+    s->rec_cv.notify_all();
+    return st;
 }
 
 gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const double* jacobian,

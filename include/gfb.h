@@ -89,6 +89,10 @@ typedef struct gfb_config {
  * one memory per global node and axis when the cells' axis coefficients
  * agree at every shared node (they are functions of the node position). */
 #define GFB_FLAG_CELL_PML 1
+/* Store snapshots as float on the device and in the pinned host ring (the
+ * reference's snapshot_precision = "float32", record.cpp:91-98, 132-139);
+ * gfb_read_record still returns doubles. */
+#define GFB_FLAG_RECORD_F32 2
 
 /* Point-force source (config.h5 /source, io.cpp:681-707). */
 typedef struct gfb_source {
@@ -200,8 +204,10 @@ gfb_status gfb_records_pending(gfb_solver* solver, int32_t* n);
  * without the leading unit axis:
  *   strain [n_rec_cell, ngll^3, 6] (xx,yy,zz,xy,xz,yz)
  *   u, v, a [n_rec_cell, ngll^3, 3]
- * Any buffer may be NULL.  The snapshot is released once every wavefield
- * has been read (or immediately when release != 0).
+ * Any buffer may be NULL (with all four NULL nothing is copied: the call
+ * only waits for the snapshot to reach host memory and can release it).
+ * The snapshot is released once every wavefield has been read (or
+ * immediately when release != 0).
  */
 gfb_status gfb_read_record(gfb_solver* solver, int32_t field, int32_t* step, double* strain,
                            double* u, double* v, double* a, int32_t release);

@@ -157,6 +157,38 @@ def test_fp32_node_and_cell_cpml_forms_agree():
             assert rel_l2(a[d][k], b[d][k]) < 1e-5
 
 
+def test_float32_snapshots_and_a_concurrent_reader():
+    """Snapshots stored as float (snapshot_precision = "float32") match the
+    double ones to float rounding; a reader thread draining snapshots while
+    gfb_advance runs receives every one, in step order."""
+    import threading
+
+    prob = layered_problem(nsteps=150)
+    a = gfb.Solver(prob, dirs=[0, 2], precision=gfb.FP32, record_slots=2)
+    b = gfb.Solver(prob, dirs=[0, 2], precision=gfb.FP32, record_slots=2, flags=gfb.FLAG_RECORD_F32)
+    got, stop = [], threading.Event()
+
+    def reader():
+        while not stop.is_set() or b.pending() > 0:
+            if b.pending() > 0:
+                got.append((b.read_record(0), b.read_record(1)))
+
+    th = threading.Thread(target=reader)
+    th.start()
+    b.advance(150)
+    b.synchronize()
+    stop.set()
+    th.join()
+    a.advance(150)
+    ref = a.drain()
+    assert [r0["step"] for r0, _ in got] == list(ref[0]["steps"])
+    for n, (r0, r1) in enumerate(got):
+        for f, r in ((0, r0), (1, r1)):
+            for k in ("u", "strain"):
+                x, y = r[k], ref[f][k][n]
+                assert np.abs(x - y).max() <= 1e-6 * np.abs(y).max() + 1e-30
+
+
 def test_node_cpml_falls_back_when_cell_coefficients_disagree():
     prob = layered_problem(nsteps=40)
     nc = prob["n_cell"]
