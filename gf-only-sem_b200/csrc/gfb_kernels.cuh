@@ -34,7 +34,8 @@
 
 namespace gfb {
 
-constexpr uint32_t kFirstTouch = 0x80000000u;
+constexpr uint32_t kFirstTouch = 0x80000000u;  // lowest colour touching the node: store
+constexpr uint32_t kLastTouch = 0x40000000u;   // highest colour touching the node: finalise
 constexpr uint32_t kNodeMask = 0x3fffffffu;
 
 // Predicted displacement and force of the time loop are stored
@@ -50,6 +51,42 @@ struct Shape {
     static constexpr int NNP = (NN + 31) / 32 * 32;
     static constexpr int EPB = NNP <= 32 ? 8 : (NNP <= 64 ? 4 : (NNP <= 128 ? 2 : 1));
     static constexpr int THREADS = NNP * EPB;
+};
+
+template <typename Real>
+struct NodeArgs {
+    long long n_node;
+    double* u;              // [node][3*n_field]
+    double* v;
+    Real* a;
+    Real* ut;               // [node][field][4]
+    const Real* force;      // [node][field][4]
+    const double* mass;     // [n_node] assembled lumped mass
+    const Real* inv_mass;   // [n_node] 1/m (FP32 path) or nullptr
+    const double* damping;  // [n_node] or nullptr
+    double dt, half_dt2, beta, gamma;
+};
+
+// C-PML at global nodes (FP32 path).
+//
+// The reference keeps C-PML memory per cell and GLL node (pml.cpp:112-149)
+// and adds each cell's term w J/rho (A1 v + A2 u + A3 m_x + A4 m_y + A5 m_z)
+// to the cell residual before assembly (pml.cpp:151-216).  At a node shared
+// by several C-PML cells the memory of an axis that is active in those
+// cells follows the same recursion m = a0 m + a1 new + a2 old with the same
+// new/old (they are node values) and the same axis coefficients (functions
+// of the node position), and A_{3+q} = 0 exactly in cells where axis q is
+// inactive.  So the memory is kept once per node and axis, and the assembled
+// term is B1 v + B2 u + B3 m_x + B4 m_y + B5 m_z with B_k = sum over the
+// node's C-PML cells of w J/rho A_k.  The host checks the axis coefficients
+// agree across cells before choosing this form.
+template <typename Real>
+struct NodePml {
+    const int* slot;     // [n_node] -1 or C-PML node slot
+    const Real* coef;    // [slot][14]: B1..B5, alpha x(3), y(3), z(3)
+    Real* mem;           // [slot][F][3]
+    Real* prev;          // [slot][F]  last step's u + c1 v
+    double c1, c2;
 };
 
 template <typename Real>
@@ -76,6 +113,12 @@ struct ElemArgs {
     const Real* src_w;    // [slot][NN]
     Real stf;
     int dir0, dir1, dir2;
+    // finalisation of the nodes whose last touching colour this is (the
+    // node update fused into the element kernel); fuse == 0 keeps the
+    // force in memory for a separate node pass
+    int fuse;
+    NodeArgs<Real> nu;
+    NodePml<Real> np;
 };
 
 template <typename Real, int NG, int NFLD>
@@ -275,6 +318,77 @@ __device__ __forceinline__ void store4(float* p, float a, float b, float c, floa
 __device__ __forceinline__ void store4(double* p, double a, double b, double c, double d) {
     reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
     reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+}
+
+// Finalise wavefield d of node g from its complete assembled force fv:
+// node C-PML term (when PML), Newmark corrector with the diagonal mass
+// (solver.cpp:52-69, legacy damping of 564-574 applied to v first) and the
+// next step's predictor (40-49), written as one 16-byte vector.
+template <typename Real, int NFLD, bool PML>
+__device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const NodePml<Real>& P, long long g,
+                                                  int d, const Real (&fv)[3]) {
+    constexpr int F = 3 * NFLD;
+    const double m = A.mass[g];
+    const double dmp = A.damping ? A.damping[g] : 0.0;
+    const Real im = A.inv_mass ? A.inv_mass[g] : Real(0);
+    int sl = -1;
+    if (PML) sl = __ldg(P.slot + g);
+    Real out[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int f = d * 3 + c;
+        const long long idx = g * F + f;
+        double vv = A.v[idx];
+        if (dmp > 0.0) vv -= dmp * vv;
+        double uu = A.u[idx];
+        const double a_old = (double)A.a[idx];
+        Real force = fv[c];
+        if (PML && sl >= 0) {
+            const Real* cf = P.coef + (size_t)sl * 14;
+            Real* mm = P.mem + ((size_t)sl * F + f) * 3;
+            Real* pv = P.prev + (size_t)sl * F + f;
+            const Real nv = (Real)(uu + P.c1 * vv);
+            const Real ov = *pv + (Real)P.c2 * (Real)a_old;
+            const Real m0 = mm[0], m1 = mm[1], m2 = mm[2];
+            force += cf[0] * (Real)vv + cf[1] * (Real)uu + cf[2] * m0 + cf[3] * m1 + cf[4] * m2;
+            if (cf[2] != Real(0)) mm[0] = cf[5] * m0 + cf[6] * nv + cf[7] * ov;
+            if (cf[3] != Real(0)) mm[1] = cf[8] * m1 + cf[9] * nv + cf[10] * ov;
+            if (cf[4] != Real(0)) mm[2] = cf[11] * m2 + cf[12] * nv + cf[13] * ov;
+            *pv = nv;
+        }
+        double a_new;
+        if (m <= 0.0) {
+            a_new = 0.0;
+        } else {
+            a_new = A.inv_mass ? (double)(force * im) : (double)force / m;
+            a_new = (double)(Real)a_new;
+            uu += A.dt * vv + A.dt * A.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
+            vv += A.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
+        }
+        A.u[idx] = uu;
+        A.v[idx] = vv;
+        A.a[idx] = (Real)a_new;
+        out[c] = (Real)(uu + A.dt * vv + A.half_dt2 * a_new);
+    }
+    store4(A.ut + ((size_t)g * NFLD + d) * 4, out[0], out[1], out[2], Real(0));
+}
+
+// Separate node pass (used when the element kernel does not finalise nodes):
+// one thread per (node, wavefield), the wavefields of a node in adjacent
+// threads, so a warp streams contiguous u, v, a and force/prediction
+// vectors and reads each node's mass / C-PML slot once.
+template <typename Real, int NFLD, bool PML>
+__global__ void node_update_kernel(NodeArgs<Real> A, NodePml<Real> P) {
+    const long long total = A.n_node * NFLD;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const long long g = t / NFLD;
+        const int d = (int)(t - g * NFLD);
+        Real fv4[4];
+        load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv4);
+        const Real fv[3] = {fv4[0], fv4[1], fv4[2]};
+        update_node_field<Real, NFLD, PML>(A, P, g, d, fv);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -558,117 +672,25 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
         if (active) {
             const uint32_t g = gword & kNodeMask;
             const bool first = gword & kFirstTouch;
+            // the highest colour touching a node completes its force here and
+            // finalises it: no cell reads the node later in this step
+            const bool fin = A.fuse && (gword & kLastTouch);
 #pragma unroll
             for (int d = 0; d < NFLD; ++d) {
-                Real* out = A.force + ((size_t)g * NFLD + d) * 4;
-                if (first) {
-                    store4(out, r[d][0], r[d][1], r[d][2], Real(0));
+                Real fo[4] = {Real(0), Real(0), Real(0), Real(0)};
+                if (!first) load4(geo + (p * NFLD + d) * 4, fo);
+                if (fin) {
+                    const Real fv[3] = {fo[0] + r[d][0], fo[1] + r[d][1], fo[2] + r[d][2]};
+                    if (A.np.slot) update_node_field<Real, NFLD, true>(A.nu, A.np, g, d, fv);
+                    else update_node_field<Real, NFLD, false>(A.nu, A.np, g, d, fv);
                 } else {
-                    Real fo[4];
-                    load4(geo + (p * NFLD + d) * 4, fo);
-                    store4(out, fo[0] + r[d][0], fo[1] + r[d][1], fo[2] + r[d][2], Real(0));
+                    store4(A.force + ((size_t)g * NFLD + d) * 4, fo[0] + r[d][0], fo[1] + r[d][1], fo[2] + r[d][2],
+                           Real(0));
                 }
             }
         }
     }
     cp_async_wait_all();
-}
-
-template <typename Real>
-struct NodeArgs {
-    long long n_node;
-    double* u;              // [node][3*n_field]
-    double* v;
-    Real* a;
-    Real* ut;               // [node][field][4]
-    const Real* force;      // [node][field][4]
-    const double* mass;     // [n_node] assembled lumped mass
-    const Real* inv_mass;   // [n_node] 1/m (FP32 path) or nullptr
-    const double* damping;  // [n_node] or nullptr
-    double dt, half_dt2, beta, gamma;
-};
-
-// C-PML at global nodes (FP32 path).
-//
-// The reference keeps C-PML memory per cell and GLL node (pml.cpp:112-149)
-// and adds each cell's term w J/rho (A1 v + A2 u + A3 m_x + A4 m_y + A5 m_z)
-// to the cell residual before assembly (pml.cpp:151-216).  At a node shared
-// by several C-PML cells the memory of an axis that is active in those
-// cells follows the same recursion m = a0 m + a1 new + a2 old with the same
-// new/old (they are node values) and the same axis coefficients (functions
-// of the node position), and A_{3+q} = 0 exactly in cells where axis q is
-// inactive.  So the memory is kept once per node and axis, and the assembled
-// term is B1 v + B2 u + B3 m_x + B4 m_y + B5 m_z with B_k = sum over the
-// node's C-PML cells of w J/rho A_k.  The host checks the axis coefficients
-// agree across cells before choosing this form.
-template <typename Real>
-struct NodePml {
-    const int* slot;     // [n_node] -1 or C-PML node slot
-    const Real* coef;    // [slot][14]: B1..B5, alpha x(3), y(3), z(3)
-    Real* mem;           // [slot][F][3]
-    Real* prev;          // [slot][F]  last step's u + c1 v
-    double c1, c2;
-};
-
-// One thread per (node, wavefield), the wavefields of a node in adjacent
-// threads, so a warp streams contiguous u, v, a and force/prediction
-// vectors and reads each node's mass / C-PML slot once: node C-PML term
-// (when P.slot), Newmark corrector (solver.cpp:52-69, legacy damping of
-// 564-574 applied to v first) and the next step's predictor (40-49).
-template <typename Real, int NFLD, bool PML>
-__global__ void node_update_kernel(NodeArgs<Real> A, NodePml<Real> P) {
-    constexpr int F = 3 * NFLD;
-    const long long total = A.n_node * NFLD;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
-        const long long g = t / NFLD;
-        const int d = (int)(t - g * NFLD);
-        const double m = A.mass[g];
-        const double dmp = A.damping ? A.damping[g] : 0.0;
-        const Real im = A.inv_mass ? A.inv_mass[g] : Real(0);
-        Real fv[4];
-        load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv);
-        int sl = -1;
-        if (PML) sl = __ldg(P.slot + g);
-        Real out[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const int f = d * 3 + c;
-            const long long idx = g * F + f;
-            double vv = A.v[idx];
-            if (dmp > 0.0) vv -= dmp * vv;
-            double uu = A.u[idx];
-            const double a_old = (double)A.a[idx];
-            Real force = fv[c];
-            if (PML && sl >= 0) {
-                const Real* cf = P.coef + (size_t)sl * 14;
-                Real* mm = P.mem + ((size_t)sl * F + f) * 3;
-                Real* pv = P.prev + (size_t)sl * F + f;
-                const Real nv = (Real)(uu + P.c1 * vv);
-                const Real ov = *pv + (Real)P.c2 * (Real)a_old;
-                const Real m0 = mm[0], m1 = mm[1], m2 = mm[2];
-                force += cf[0] * (Real)vv + cf[1] * (Real)uu + cf[2] * m0 + cf[3] * m1 + cf[4] * m2;
-                if (cf[2] != Real(0)) mm[0] = cf[5] * m0 + cf[6] * nv + cf[7] * ov;
-                if (cf[3] != Real(0)) mm[1] = cf[8] * m1 + cf[9] * nv + cf[10] * ov;
-                if (cf[4] != Real(0)) mm[2] = cf[11] * m2 + cf[12] * nv + cf[13] * ov;
-                *pv = nv;
-            }
-            double a_new;
-            if (m <= 0.0) {
-                a_new = 0.0;
-            } else {
-                a_new = A.inv_mass ? (double)(force * im) : (double)force / m;
-                a_new = (double)(Real)a_new;
-                uu += A.dt * vv + A.dt * A.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
-                vv += A.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
-            }
-            A.u[idx] = uu;
-            A.v[idx] = vv;
-            A.a[idx] = (Real)a_new;
-            out[c] = (Real)(uu + A.dt * vv + A.half_dt2 * a_new);
-        }
-        store4(A.ut + ((size_t)g * NFLD + d) * 4, out[0], out[1], out[2], Real(0));
-    }
 }
 
 // Predictor only (start of a run or after a state overwrite).

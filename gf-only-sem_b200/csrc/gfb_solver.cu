@@ -136,6 +136,7 @@ struct gfb_solver {
     int stride = 0;
     int dirs[3] = {0, 1, 2};
     int flags = 0;
+    bool fuse = false;  // node update in the element kernel's last colour
     int step = 0;
     std::vector<int> colour_begin;  // [n_colour+1] device cell ranges
     std::vector<double> stf;
@@ -236,6 +237,32 @@ gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
 // kernel dispatch
 // ---------------------------------------------------------------------------
 
+template <typename Real>
+void node_args(const gfb_solver* s, gfb::NodeArgs<Real>& A, gfb::NodePml<Real>& P) {
+    A.n_node = s->n_node;
+    A.u = s->u;
+    A.v = s->v;
+    A.a = static_cast<Real*>(s->a);
+    A.ut = static_cast<Real*>(s->ut);
+    A.force = static_cast<const Real*>(s->force);
+    A.mass = s->mass;
+    A.inv_mass = static_cast<const Real*>(s->inv_mass);
+    A.damping = s->has_damping ? s->damping : nullptr;
+    A.dt = s->dt;
+    A.beta = 0.0;
+    A.gamma = 0.5;
+    A.half_dt2 = 0.5 * s->dt * s->dt * (1.0 - 2.0 * A.beta);
+    P = gfb::NodePml<Real>{};
+    if (s->node_pml) {
+        P.slot = s->npml_slot;
+        P.coef = static_cast<const Real*>(s->npml_coef);
+        P.mem = static_cast<Real*>(s->npml_mem);
+        P.prev = static_cast<Real*>(s->npml_prev);
+        P.c1 = s->c1;
+        P.c2 = s->c2;
+    }
+}
+
 template <typename Real, int NG, int NFLD>
 gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     using S = gfb::PipeShape<Real, NG, NFLD>;
@@ -265,6 +292,8 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     A.dir0 = s->dirs[0];
     A.dir1 = s->dirs[1];
     A.dir2 = s->dirs[2];
+    A.fuse = s->fuse ? 1 : 0;
+    node_args(s, A.nu, A.np);
     const int n = A.e_end - A.e_begin;
     const int groups = (n + S::EPB - 1) / S::EPB;
     const int blocks = std::max(1, std::min(groups, s->pipe_blocks));
@@ -358,32 +387,11 @@ int grid_for(long long n, int threads) {
 template <typename Real, int NFLD>
 gfb_status launch_node_f(gfb_solver* s) {
     gfb::NodeArgs<Real> A;
-    A.n_node = s->n_node;
-    A.u = s->u;
-    A.v = s->v;
-    A.a = static_cast<Real*>(s->a);
-    A.ut = static_cast<Real*>(s->ut);
-    A.force = static_cast<const Real*>(s->force);
-    A.mass = s->mass;
-    A.inv_mass = static_cast<const Real*>(s->inv_mass);
-    A.damping = s->has_damping ? s->damping : nullptr;
-    A.dt = s->dt;
-    A.beta = 0.0;
-    A.gamma = 0.5;
-    A.half_dt2 = 0.5 * s->dt * s->dt * (1.0 - 2.0 * A.beta);
-    gfb::NodePml<Real> P{};
+    gfb::NodePml<Real> P;
+    node_args(s, A, P);
     const int grid = grid_for((long long)s->n_node * NFLD, 256);
-    if (s->node_pml) {
-        P.slot = s->npml_slot;
-        P.coef = static_cast<const Real*>(s->npml_coef);
-        P.mem = static_cast<Real*>(s->npml_mem);
-        P.prev = static_cast<Real*>(s->npml_prev);
-        P.c1 = s->c1;
-        P.c2 = s->c2;
-        gfb::node_update_kernel<Real, NFLD, true><<<grid, 256, 0, s->stream>>>(A, P);
-    } else {
-        gfb::node_update_kernel<Real, NFLD, false><<<grid, 256, 0, s->stream>>>(A, P);
-    }
+    if (s->node_pml) gfb::node_update_kernel<Real, NFLD, true><<<grid, 256, 0, s->stream>>>(A, P);
+    else gfb::node_update_kernel<Real, NFLD, false><<<grid, 256, 0, s->stream>>>(A, P);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -740,7 +748,8 @@ gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
     for (int c = 0; c < n_colour; ++c)
         if ((st = launch_elem(s, c, stf))) return st;
     if (ev) CU(cudaEventRecord(ev[1], s->stream));
-    if ((st = launch_node(s))) return st;
+    if (!s->fuse)
+        if ((st = launch_node(s))) return st;
     if (ev) CU(cudaEventRecord(ev[2], s->stream));
     if (s->stride > 0 && s->n_rec > 0 && step % s->stride == 0) {
         // round-robin slot; an unread snapshot still in it moves to pageable
@@ -813,6 +822,7 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     s->has_cpml = m->pml_coef_abar != nullptr;
     s->flags = c->flags;
     s->rec_f32 = (c->flags & GFB_FLAG_RECORD_F32) != 0;
+    s->fuse = (c->flags & GFB_FLAG_FUSED_NODE) != 0;
     s->n_rec = m->n_rec_cell;
     s->slots = std::max(1, c->record_slots);
     const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
@@ -875,8 +885,9 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
             inv_perm[e] = ed;
         }
     }
-    // device ibool with the first-touch bit: the lowest colour touching a
-    // node stores, later colours add
+    // device ibool with the first/last-touch bits: the lowest colour
+    // touching a node stores its force, later colours add, the highest
+    // colour finalises the node
     std::vector<uint32_t> ibool_dev((size_t)P);
     parallel_for(m->n_cell, [&](long long e0, long long e1) {
         for (long long ed = e0; ed < e1; ++ed) {
@@ -884,7 +895,8 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
             for (int p = 0; p < nn; ++p) {
                 const uint32_t g = (uint32_t)m->ibool[e * nn + p];
                 const bool first = __builtin_ctzll(used[g]) == colour[e];
-                ibool_dev[ed * nn + p] = g | (first ? gfb::kFirstTouch : 0u);
+                const bool last = 63 - __builtin_clzll(used[g]) == colour[e];
+                ibool_dev[ed * nn + p] = g | (first ? gfb::kFirstTouch : 0u) | (last ? gfb::kLastTouch : 0u);
             }
         }
     });

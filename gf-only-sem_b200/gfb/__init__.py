@@ -25,6 +25,7 @@ HEADER_PATH = os.path.join(os.path.dirname(PKG_ROOT), "include", "gfb.h")
 FP64, FP32 = 0, 1
 FLAG_CELL_PML = 1
 FLAG_RECORD_F32 = 2
+FLAG_FUSED_NODE = 4
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

@@ -93,6 +93,11 @@ typedef struct gfb_config {
  * reference's snapshot_precision = "float32", record.cpp:91-98, 132-139);
  * gfb_read_record still returns doubles. */
 #define GFB_FLAG_RECORD_F32 2
+/* Update each node in the epilogue of the element kernel of the highest
+ * colour touching it instead of in a separate node pass (same results).
+ * Slower on B200 as laid out today: the epilogue's scattered per-node
+ * accesses cost far more L1 transactions than the contiguous node pass. */
+#define GFB_FLAG_FUSED_NODE 4
 
 /* Point-force source (config.h5 /source, io.cpp:681-707). */
 typedef struct gfb_source {

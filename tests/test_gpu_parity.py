@@ -210,6 +210,25 @@ def test_node_cpml_falls_back_when_cell_coefficients_disagree():
 
 
 @pytest.mark.parametrize("prec", [gfb.FP64, gfb.FP32])
+def test_fused_node_update_equals_separate_pass(prec):
+    """Finalising each node in the element kernel of the highest colour that
+    touches it computes the same expressions as the separate node pass."""
+    prob = layered_problem(nsteps=70)
+    runs = []
+    for flags in (0, gfb.FLAG_FUSED_NODE):
+        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=prec, flags=flags)
+        s.advance(70)
+        runs.append((s.drain(), [s.state(f) for f in range(3)]))
+        s.close()
+    (a, sa), (b, sb) = runs
+    for f in range(3):
+        for k in ("strain", "u", "v", "a"):
+            np.testing.assert_array_equal(a[f][k], b[f][k])
+        for x, y in zip(sa[f], sb[f]):
+            np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec", [gfb.FP64, gfb.FP32])
 def test_assembly_is_bit_reproducible(prec):
     prob = layered_problem(nsteps=60)
     out = []
