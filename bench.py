@@ -72,6 +72,21 @@ def build_workload(name: str):
                               record_depth_max_m=w["depth"])
 
 
+def max_over_ranks(seconds: float, dist, device: str) -> float:
+    """Slowest rank's timed region (replicas run independently; the job
+    finishes with the slowest)."""
+    import torch
+
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_units(n_cell: int, n_field: int, steps: int, world: int) -> int:
+    """GLL-point updates done by all replicas in the timed region."""
+    return n_cell * 125 * n_field * steps * world
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -199,6 +214,30 @@ def committed_traffic():
             return json.load(f)
     except Exception:
         return None
+
+
+def fp64_plain_sample(prob, device, args, fp32_value_per_gpu):
+    """The plain FP64 single-direction GPU path on the same workload (the
+    denominator of the FP32-batched speed-up): one wavefield, FP64 state and
+    arithmetic, per-cell C-PML as the reference lays it out."""
+    import gfb
+
+    s = gfb.Solver(prob, dirs=[0], precision=gfb.FP64, device=device, record_slots=8,
+                   flags=gfb.FLAG_RECORD_F32 if args.record_f32 else 0)
+    s.advance(args.warmup)
+    s.drain()
+    s.synchronize()
+    n = max(20, args.steps // 4)
+    consumer = RecordConsumer(s)
+    consumer.start()
+    ms_e, ms_n, ms_r = s.advance_profiled(n)
+    consumer.stop()
+    s.close()
+    ms = (ms_e + ms_n + ms_r) / n
+    val = prob["n_cell"] * 125 * 1 / (ms / 1e3)
+    return {"value": val, "unit": UNIT, "steps": n, "ms_per_step": ms,
+            "phases_ms_per_step": {"element": ms_e / n, "node": ms_n / n, "record": ms_r / n},
+            "fp32_batched_over_fp64_plain": fp32_value_per_gpu / val}
 
 
 def cpu_baseline_sample(prob, seconds_target=20.0):
@@ -346,12 +385,8 @@ def run_gfb(args):
     dev_ms = ms_elem + ms_node + ms_rec
     elapsed = dev_ms / 1e3
     if dist:
-        import torch
-
-        t = torch.tensor([elapsed], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-    units = prob["n_cell"] * 125 * len(dirs) * args.steps * world
+        elapsed = max_over_ranks(elapsed, dist, f"cuda:{local}")
+    units = replica_units(prob["n_cell"], len(dirs), args.steps, world)
     value = units / elapsed
     s.drain()
     s.close()
@@ -402,6 +437,8 @@ def run_gfb(args):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if rank == 0 and not args.no_plain:
+        line["fp64_plain"] = fp64_plain_sample(prob, device, args, value / world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(prob)
     if dist:
@@ -422,6 +459,7 @@ def main():
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 single-direction comparison")
     ap.add_argument("--record-f64", dest="record_f32", action="store_false",
                     help="snapshots in double (default: float, the reference example's snapshot_precision)")
     args = ap.parse_args()
