@@ -351,9 +351,13 @@ def run_gfb(args):
     prec = gfb.FP32 if args.precision == "fp32" else gfb.FP64
     dirs = [0, 1, 2][: args.fields]
     prob = build_workload(args.workload)
-    flags = gfb.FLAG_RECORD_F32 if args.record_f32 else 0
+    flags = (gfb.FLAG_RECORD_F32 if args.record_f32 else 0) | (gfb.FLAG_POINT_KERNEL if args.point_kernel else 0)
     s = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8, flags=flags)
     info = s.info()
+    if prec == gfb.FP32 and not args.point_kernel:
+        kname = f"elem_col_kernel<5,{len(dirs)}>"
+    else:
+        kname = f"elem_pipe_kernel<{'float' if prec == gfb.FP32 else 'double'},5,{len(dirs)}>"
     s.advance(args.warmup)
     s.drain()
     s.synchronize()
@@ -426,7 +430,7 @@ def run_gfb(args):
                                "record": ms_rec / args.steps, "wall": wall / args.steps * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "kernel": "elem_step_kernel (all colour launches of a step)",
+                     "kernel": f"{kname} (all colour launches of a step)",
                      "algorithmic_bytes_per_step": eb,
                      "traffic": (traffic or {}).get("bytes_per_step") if traffic else None},
         "roofline_node": {"achieved": nb / (ms_node / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -460,6 +464,8 @@ def main():
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 single-direction comparison")
+    ap.add_argument("--point-kernel", action="store_true",
+                    help="FP32 path with the thread-per-point element kernel instead of the line kernel")
     ap.add_argument("--record-f64", dest="record_f32", action="store_false",
                     help="snapshots in double (default: float, the reference example's snapshot_precision)")
     args = ap.parse_args()

@@ -693,6 +693,288 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
     cp_async_wait_all();
 }
 
+// ---------------------------------------------------------------------------
+// elem_col_kernel: element/assembly kernel with one thread per
+// (cell, wavefield, xi-line).
+//
+// The thread-per-point kernel above reads 15 neighbour vectors per point for
+// the gradient and 15 flux vectors for the divergence, all from shared
+// memory, and shared-memory bandwidth is what bounds it.  Here a thread owns
+// the NG points (i = 0..NG-1, j, k) of one xi-line of one wavefield: the xi
+// contractions of the gradient and of the divergence run on values held in
+// registers, and only the eta and zeta neighbours go through shared memory,
+// as one float per component (structure-of-arrays, no padding lane).  The
+// per-(cell, wavefield) arrays are SP floats apart with SP = NG*NG (mod 32),
+// so that the eta/zeta reads of a warp that spans two or three of them fall
+// in distinct banks.  The D entries indexed by the loop counter come from
+// the kernel parameters (constant bank); those indexed by the thread's own j
+// and k are kept in registers.
+//
+// Pipelining: the geometry of the next group and the node table of the one
+// after are cp.async copies into rotating shared stages; the next group's
+// predicted-displacement vectors and this group's old force vectors are
+// register loads issued a phase ahead of their use.
+// ---------------------------------------------------------------------------
+
+template <int NG, int NFLD>
+struct ColShape {
+    static constexpr int NN = NG * NG * NG;
+    static constexpr int NG2 = NG * NG;
+    static constexpr int NNP = (NN + 31) / 32 * 32;
+    static constexpr int EPB = (150 / (NFLD * NG2)) > 0 ? 150 / (NFLD * NG2) : 1;  // cells per group
+    static constexpr int GR = EPB * NFLD;                 // (cell, wavefield) lines per group
+    static constexpr int ACTIVE = GR * NG2;               // threads with work
+    static constexpr int THREADS = (ACTIVE + 31) / 32 * 32;
+    static constexpr int SP = NN + ((NG2 - NN) % 32 + 32) % 32;  // >= NN, == NG2 (mod 32)
+    static constexpr int GEO_B = 12 * NN * 4;
+    static constexpr int GEO_W = GEO_B / 4;
+    static constexpr int GEO_SLOT = GEO_B + 4 * (((24 - GEO_W) % 32 + 32) % 32 / 4 * 4);
+    static constexpr int IB_B = NNP * 4;
+    static constexpr int ARR = 3 * GR * SP;               // floats of one [3][GR][SP] array
+    static constexpr int SMEM = 2 * EPB * GEO_SLOT + 3 * EPB * IB_B + (3 * ARR + 64) * 4;
+    static_assert(GEO_B % 16 == 0 && GEO_SLOT % 16 == 0 && IB_B % 16 == 0, "16-byte copies");
+};
+
+struct ColArgs {
+    int e_begin, e_end, n_groups;
+    const uint32_t* ibool_padded;  // [cell][NNP]
+    const float* geom;             // [cell][12][NN]
+    const float* ut;               // [node][NFLD][4]
+    float* force;                  // [node][NFLD][4]
+    const float* dmat;             // [NG*NG]
+    const int* src_head;
+    const int* src_next;
+    const float* src_w;
+    float stf;
+    int dir[3];
+    float D[36];                   // D[i*NG+s], read with compile-time indices only
+};
+
+template <int NG, int NFLD>
+__global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kernel(ColArgs A) {
+    using S = ColShape<NG, NFLD>;
+    constexpr int NN = S::NN, NG2 = S::NG2, EPB = S::EPB, GR = S::GR, SP = S::SP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* gbase = smem_raw;
+    unsigned char* ibase = gbase + 2 * EPB * S::GEO_SLOT;
+    float* us = reinterpret_cast<float*>(ibase + 3 * EPB * S::IB_B);  // [3][GR][SP] displacement
+    float* fe = us + S::ARR;                                          // [3][GR][SP] eta flux
+    float* fz = fe + S::ARR;                                          // [3][GR][SP] zeta flux
+    float* sD = fz + S::ARR;
+
+    const int tid = threadIdx.x;
+    const bool lane_ok = tid < S::ACTIVE;
+    const int line = lane_ok ? tid / NG2 : 0;  // (cell, wavefield) line of this thread
+    const int col = lane_ok ? tid - line * NG2 : 0;
+    const int cl = line / NFLD, fld = line - cl * NFLD;
+    const int j = col / NG, k = col - j * NG;
+    const int dir = fld == 0 ? A.dir[0] : (fld == 1 ? A.dir[1] : A.dir[2]);
+    if (tid < NG2) sD[tid] = A.dmat[tid];
+    __syncthreads();
+    float Dj[NG], Dk[NG], Tj[NG], Tk[NG];
+#pragma unroll
+    for (int s = 0; s < NG; ++s) {
+        Dj[s] = sD[j * NG + s];
+        Dk[s] = sD[k * NG + s];
+        Tj[s] = sD[s * NG + j];
+        Tk[s] = sD[s * NG + k];
+    }
+
+    auto geo_of = [&](int st, int c) -> const float* {
+        return reinterpret_cast<const float*>(gbase + (st * EPB + c) * S::GEO_SLOT);
+    };
+    auto ib_of = [&](int st, int c) -> const uint32_t* {
+        return reinterpret_cast<const uint32_t*>(ibase + (st * EPB + c) * S::IB_B);
+    };
+    auto issue_ib = [&](int grp, int st) {
+        constexpr int CI = S::IB_B / 16;
+        for (int q = tid; q < EPB * CI; q += S::THREADS) {
+            const int c = q / CI, r = q - c * CI;
+            const int e = A.e_begin + grp * EPB + c;
+            if (e < A.e_end)
+                cp_async16(ibase + (st * EPB + c) * S::IB_B + r * 16,
+                           reinterpret_cast<const unsigned char*>(A.ibool_padded) + (size_t)e * S::IB_B + r * 16);
+        }
+    };
+    auto issue_geo = [&](int grp, int st) {
+        constexpr int CG = S::GEO_B / 16;
+        for (int q = tid; q < EPB * CG; q += S::THREADS) {
+            const int c = q / CG, r = q - c * CG;
+            const int e = A.e_begin + grp * EPB + c;
+            if (e < A.e_end)
+                cp_async16(gbase + (st * EPB + c) * S::GEO_SLOT + r * 16,
+                           reinterpret_cast<const unsigned char*>(A.geom) + (size_t)e * S::GEO_B + r * 16);
+        }
+    };
+    // node words of this thread's line of group grp (node table in stage st)
+    auto line_nodes = [&](int grp, int st, uint32_t (&w)[NG]) -> bool {
+        const bool ok = lane_ok && grp < A.n_groups && A.e_begin + grp * EPB + cl < A.e_end;
+#pragma unroll
+        for (int i = 0; i < NG; ++i) w[i] = ok ? ib_of(st, cl)[i * NG2 + col] : 0u;
+        return ok;
+    };
+    auto load_vectors = [&](const uint32_t (&w)[NG], bool ok, float4 (&v)[NG]) {
+#pragma unroll
+        for (int i = 0; i < NG; ++i)
+            v[i] = ok ? __ldg(reinterpret_cast<const float4*>(A.ut) + (size_t)(w[i] & kNodeMask) * NFLD + fld)
+                      : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+
+    const int G = gridDim.x;
+    const int grp0 = blockIdx.x;
+    if (grp0 < A.n_groups) issue_ib(grp0, 0);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    uint32_t nw[NG];
+    float4 pre[NG];
+    bool pre_ok = line_nodes(grp0, 0, nw);
+    load_vectors(nw, pre_ok, pre);
+    if (grp0 < A.n_groups) issue_geo(grp0, 0);
+    if (grp0 + G < A.n_groups) issue_ib(grp0 + G, 1);
+    cp_async_commit();
+
+    const int ubase = line * SP + col;        // + c*GR*SP + i*NG2
+    const int ebase = line * SP + col - j * NG;  // + s*NG  (eta line: i*NG2 + s*NG + k)
+    const int zbase = line * SP + j * NG;        // + s     (zeta line: i*NG2 + j*NG + s)
+
+    int it = 0;
+    for (int grp = grp0; grp < A.n_groups; grp += G, ++it) {
+        const bool act = pre_ok;
+        const int e = A.e_begin + grp * EPB + cl;
+        uint32_t cw[NG];
+        float u0[NG], u1[NG], u2[NG];
+#pragma unroll
+        for (int i = 0; i < NG; ++i) {
+            cw[i] = nw[i];
+            u0[i] = pre[i].x;
+            u1[i] = pre[i].y;
+            u2[i] = pre[i].z;
+            if (act) {
+                us[0 * GR * SP + ubase + i * NG2] = u0[i];
+                us[1 * GR * SP + ubase + i * NG2] = u1[i];
+                us[2 * GR * SP + ubase + i * NG2] = u2[i];
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();  // displacement of this group, its geometry, the next node table
+        const int nx = grp + G;
+        if (nx < A.n_groups) issue_geo(nx, (it + 1) & 1);
+        if (nx + G < A.n_groups) issue_ib(nx + G, (it + 2) % 3);
+        cp_async_commit();
+        pre_ok = line_nodes(nx, (it + 1) % 3, nw);
+        load_vectors(nw, pre_ok, pre);
+
+        // gradient, stress and the three fluxes at each point of the line
+        float fx0[NG], fx1[NG], fx2[NG];
+        const float* geo = geo_of(it & 1, cl);
+#pragma unroll
+        for (int i = 0; i < NG; ++i) {
+            fx0[i] = fx1[i] = fx2[i] = 0.f;
+            if (!act) continue;
+            const int p = i * NG2 + col;
+            float dd[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) dd[q] = geo[q * NN + p];
+            const float jw = geo[9 * NN + p], lam = geo[10 * NN + p], mu = geo[11 * NN + p];
+            float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int s = 0; s < NG; ++s) {
+                const float Di = A.D[i * NG + s];
+                gx[0] += Di * u0[s];
+                gx[1] += Di * u1[s];
+                gx[2] += Di * u2[s];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float* uc = us + c * GR * SP + i * NG2;
+#pragma unroll
+                for (int s = 0; s < NG; ++s) {
+                    gy[c] += Dj[s] * uc[ebase + s * NG];
+                    gz[c] += Dk[s] * uc[zbase + s];
+                }
+            }
+            float st0 = 0.f, st1 = 0.f, st2 = 0.f, st3 = 0.f, st4 = 0.f, st5 = 0.f;
+            if (mu > 0.f) {  // element_cpu.cpp:42-43: mu <= 0 adds nothing
+                float gr[3][3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    gr[c][0] = gx[c] * dd[0] + gy[c] * dd[1] + gz[c] * dd[2];
+                    gr[c][1] = gx[c] * dd[3] + gy[c] * dd[4] + gz[c] * dd[5];
+                    gr[c][2] = gx[c] * dd[6] + gy[c] * dd[7] + gz[c] * dd[8];
+                }
+                const float tr = gr[0][0] + gr[1][1] + gr[2][2];
+                const float m2 = 2.f * mu;
+                st0 = m2 * gr[0][0] + lam * tr;
+                st1 = m2 * gr[1][1] + lam * tr;
+                st2 = m2 * gr[2][2] + lam * tr;
+                st3 = m2 * (0.5f * (gr[0][1] + gr[1][0]));
+                st4 = m2 * (0.5f * (gr[0][2] + gr[2][0]));
+                st5 = m2 * (0.5f * (gr[1][2] + gr[2][1]));
+            }
+            // flux along axis a: jw * sigma . (dd[a], dd[3+a], dd[6+a])
+            fx0[i] = jw * (st0 * dd[0] + st3 * dd[3] + st4 * dd[6]);
+            fx1[i] = jw * (st3 * dd[0] + st1 * dd[3] + st5 * dd[6]);
+            fx2[i] = jw * (st4 * dd[0] + st5 * dd[3] + st2 * dd[6]);
+            fe[0 * GR * SP + ubase + i * NG2] = jw * (st0 * dd[1] + st3 * dd[4] + st4 * dd[7]);
+            fe[1 * GR * SP + ubase + i * NG2] = jw * (st3 * dd[1] + st1 * dd[4] + st5 * dd[7]);
+            fe[2 * GR * SP + ubase + i * NG2] = jw * (st4 * dd[1] + st5 * dd[4] + st2 * dd[7]);
+            fz[0 * GR * SP + ubase + i * NG2] = jw * (st0 * dd[2] + st3 * dd[5] + st4 * dd[8]);
+            fz[1 * GR * SP + ubase + i * NG2] = jw * (st3 * dd[2] + st1 * dd[5] + st5 * dd[8]);
+            fz[2 * GR * SP + ubase + i * NG2] = jw * (st4 * dd[2] + st5 * dd[5] + st2 * dd[8]);
+        }
+        // old force of the nodes this colour does not touch first
+        float4 of[NG];
+#pragma unroll
+        for (int i = 0; i < NG; ++i)
+            of[i] = (act && !(cw[i] & kFirstTouch))
+                        ? *(reinterpret_cast<const float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld)
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();  // fluxes of the whole group
+        if (act) {
+            int src = (A.stf != 0.f && A.src_head) ? __ldg(A.src_head + e) : -1;
+#pragma unroll
+            for (int i = 0; i < NG; ++i) {
+                const int p = i * NG2 + col;
+                float r[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int s = 0; s < NG; ++s) {
+                    const float Ti = A.D[s * NG + i];
+                    r[0] += Ti * fx0[s];
+                    r[1] += Ti * fx1[s];
+                    r[2] += Ti * fx2[s];
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const float* ec = fe + c * GR * SP + i * NG2;
+                    const float* zc = fz + c * GR * SP + i * NG2;
+#pragma unroll
+                    for (int s = 0; s < NG; ++s) {
+                        r[c] += Tj[s] * ec[ebase + s * NG];
+                        r[c] += Tk[s] * zc[zbase + s];
+                    }
+                }
+                r[0] = -r[0];
+                r[1] = -r[1];
+                r[2] = -r[2];
+                // point force (solver.cpp:577-605)
+                for (int sl = src; sl >= 0; sl = __ldg(A.src_next + sl)) {
+                    const float w = __ldg(A.src_w + (size_t)sl * NN + p);
+                    if (w != 0.f) {
+                        const float sw = A.stf * w;
+                        if (dir == 0) r[0] += sw;
+                        else if (dir == 1) r[1] += sw;
+                        else r[2] += sw;
+                    }
+                }
+                float4* dst = reinterpret_cast<float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld;
+                *dst = make_float4(of[i].x + r[0], of[i].y + r[1], of[i].z + r[2], 0.f);
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
 // Predictor only (start of a run or after a state overwrite).
 template <typename Real>
 __global__ void predict_kernel(long long n_node, int F, const double* u, const double* v, const Real* a,

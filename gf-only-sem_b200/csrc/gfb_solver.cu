@@ -15,6 +15,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/gfb.h"
@@ -148,8 +149,10 @@ struct gfb_solver {
     uint32_t* ibool = nullptr;
     uint32_t* ibool_padded = nullptr;  // [cell][NNP] for the pipelined kernel
     int pipe_blocks = 0;               // persistent grid of the element kernel
+    int col_blocks = 0;                // persistent grid of the line kernel (FP32)
     void* geom = nullptr;
     void* dmat = nullptr;
+    float dmat_host[36] = {};          // D of the line kernel's parameters
     double *u = nullptr, *v = nullptr;
     void *a = nullptr, *ut = nullptr, *force = nullptr;
     double* mass = nullptr;
@@ -303,6 +306,40 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     return GFB_OK;
 }
 
+// The FP32 path runs the line kernel unless per-cell C-PML, the fused node
+// update or GFB_FLAG_POINT_KERNEL asks for the thread-per-point kernel.
+bool use_col_kernel(const gfb_solver* s) {
+    return s->prec == GFB_FP32 && !(s->has_cpml && !s->node_pml) && !s->fuse &&
+           !(s->flags & GFB_FLAG_POINT_KERNEL);
+}
+
+template <int NG, int NFLD>
+gfb_status launch_col_t(gfb_solver* s, int c, float stf) {
+    using S = gfb::ColShape<NG, NFLD>;
+    gfb::ColArgs A;
+    A.e_begin = s->colour_begin[c];
+    A.e_end = s->colour_begin[c + 1];
+    if (A.e_end <= A.e_begin) return GFB_OK;
+    const int n = A.e_end - A.e_begin;
+    A.n_groups = (n + S::EPB - 1) / S::EPB;
+    A.ibool_padded = s->ibool_padded;
+    A.geom = static_cast<const float*>(s->geom);
+    A.ut = static_cast<const float*>(s->ut);
+    A.force = static_cast<float*>(s->force);
+    A.dmat = static_cast<const float*>(s->dmat);
+    A.src_head = s->has_src ? s->src_head : nullptr;
+    A.src_next = s->src_next;
+    A.src_w = static_cast<const float*>(s->src_w);
+    A.stf = stf;
+    for (int d = 0; d < 3; ++d) A.dir[d] = s->dirs[d];
+    for (int q = 0; q < 36; ++q) A.D[q] = q < NG * NG ? s->dmat_host[q] : 0.f;
+    const int blocks = std::max(1, std::min(A.n_groups, s->col_blocks));
+    gfb::elem_col_kernel<NG, NFLD><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
 template <typename Real, int NG, int NFLD>
 gfb_status set_smem_t(gfb_solver* s) {
     using S = gfb::PipeShape<Real, NG, NFLD>;
@@ -314,6 +351,14 @@ gfb_status set_smem_t(gfb_solver* s) {
     CU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->device));
     if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "element kernel does not fit on an SM");
     s->pipe_blocks = per_sm * n_sm;
+    if constexpr (std::is_same<Real, float>::value) {
+        using C = gfb::ColShape<NG, NFLD>;
+        CU(cudaFuncSetAttribute(gfb::elem_col_kernel<NG, NFLD>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gfb::elem_col_kernel<NG, NFLD>, C::THREADS,
+                                                         C::SMEM));
+        if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "line element kernel does not fit on an SM");
+        s->col_blocks = per_sm * n_sm;
+    }
     return GFB_OK;
 }
 
@@ -358,7 +403,11 @@ gfb_status dispatch(int ng, int nfld, Args... args) {
 
 template <typename Real, int NG, int NFLD>
 struct ElemOp {
-    static gfb_status run(gfb_solver* s, int c, double stf) { return launch_elem_t<Real, NG, NFLD>(s, c, (Real)stf); }
+    static gfb_status run(gfb_solver* s, int c, double stf) {
+        if constexpr (std::is_same<Real, float>::value)
+            if (use_col_kernel(s)) return launch_col_t<NG, NFLD>(s, c, (float)stf);
+        return launch_elem_t<Real, NG, NFLD>(s, c, (Real)stf);
+    }
 };
 template <typename Real, int NG, int NFLD>
 struct SmemOp {
@@ -565,6 +614,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     {
         std::vector<Real> d(D.size());
         for (size_t i = 0; i < D.size(); ++i) d[i] = (Real)D[i];
+        for (size_t i = 0; i < D.size() && i < 36; ++i) s->dmat_host[i] = (float)D[i];
         if ((st = upload(s, &s->dmat, d))) return st;
     }
     const long long nF = (long long)s->n_node * s->F;

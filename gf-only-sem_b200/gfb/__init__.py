@@ -26,6 +26,7 @@ FP64, FP32 = 0, 1
 FLAG_CELL_PML = 1
 FLAG_RECORD_F32 = 2
 FLAG_FUSED_NODE = 4
+FLAG_POINT_KERNEL = 8
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

@@ -98,6 +98,10 @@ typedef struct gfb_config {
  * Slower on B200 as laid out today: the epilogue's scattered per-node
  * accesses cost far more L1 transactions than the contiguous node pass. */
 #define GFB_FLAG_FUSED_NODE 4
+/* Run the FP32 path with the thread-per-GLL-point element kernel instead of
+ * the thread-per-xi-line kernel (same arithmetic, different summation order;
+ * for comparisons). */
+#define GFB_FLAG_POINT_KERNEL 8
 
 /* Point-force source (config.h5 /source, io.cpp:681-707). */
 typedef struct gfb_source {

@@ -215,7 +215,9 @@ def test_fused_node_update_equals_separate_pass(prec):
     touches it computes the same expressions as the separate node pass."""
     prob = layered_problem(nsteps=70)
     runs = []
-    for flags in (0, gfb.FLAG_FUSED_NODE):
+    # the fused update lives in the thread-per-point kernel; compare with the
+    # same kernel and a separate node pass
+    for flags in (gfb.FLAG_POINT_KERNEL, gfb.FLAG_FUSED_NODE):
         s = gfb.Solver(prob, dirs=[0, 1, 2], precision=prec, flags=flags)
         s.advance(70)
         runs.append((s.drain(), [s.state(f) for f in range(3)]))
@@ -226,6 +228,41 @@ def test_fused_node_update_equals_separate_pass(prec):
             np.testing.assert_array_equal(a[f][k], b[f][k])
         for x, y in zip(sa[f], sb[f]):
             np.testing.assert_array_equal(x, y)
+
+
+def test_fp32_line_and_point_kernels_agree():
+    """The FP32 path's thread-per-xi-line element kernel and the thread-per-
+    point kernel compute the same sums in a different order: traces agree to
+    FP32 rounding and both stay within 1e-4 of the oracle."""
+    prob = layered_problem(nsteps=200)
+    n = prob["nsteps"]
+    runs = []
+    for flags in (0, gfb.FLAG_POINT_KERNEL):
+        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, flags=flags)
+        s.advance(n)
+        runs.append(s.drain())
+        s.close()
+    line, point = runs
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(line[d], ref, FP32_TOL, f"line kernel field {d}")
+        compare_runs(point[d], ref, FP32_TOL, f"point kernel field {d}")
+        for k in ("u", "strain"):
+            assert rel_l2(line[d][k], point[d][k]) < 1e-5
+
+
+@pytest.mark.parametrize("order,dirs", [(2, [1]), (3, [0, 2]), (5, [0, 1, 2]), (4, [2])])
+def test_fp32_line_kernel_orders_and_field_counts(order, dirs):
+    """Every (order, wavefield count) shape of the line kernel: its cells per
+    group and thread count change with both."""
+    n = 80
+    prob = layered_problem(nsteps=n, order=order)
+    s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
+    s.advance(n)
+    snaps = s.drain()
+    for f, d in enumerate(dirs):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(snaps[f], ref, FP32_TOL, f"order {order} field {d}")
 
 
 @pytest.mark.parametrize("prec", [gfb.FP64, gfb.FP32])
