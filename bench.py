@@ -54,6 +54,10 @@ WORKLOADS = {
                                nsteps=2000, stride=10, depth=500.0),
 }
 
+# 32 independent models of uneven size stepped together
+BATCH = dict(n_model=32, seed=4, d=250.0, pml=4, nmin=(16, 16, 8), nmax=(48, 48, 24), f0=(1.0, 3.0),
+             steps=(1000, 3000), stride=50)
+
 METRIC = "GLL-point updates/s (FP32 batched x/y/z, 1 B200)"
 UNIT = "GLL-pt/s"
 
@@ -70,6 +74,100 @@ def build_workload(name: str):
         mat = mesh.homogeneous()
     return mesh.build_problem(spec, mat, np.array(w["src"]), nsteps=w["nsteps"], snapshot_stride=w["stride"],
                               record_depth_max_m=w["depth"])
+
+
+def batch_specs(seed: int = BATCH["seed"], n_model: int = BATCH["n_model"]):
+    """Seeded descriptions of the uneven models: cells per axis, halfspace or
+    layered material, source position, Ricker frequency and step count."""
+    rng = np.random.default_rng(seed)
+    d, pml = BATCH["d"], BATCH["pml"]
+    out = []
+    for k in range(n_model):
+        nx, ny, nz = (int(rng.integers(lo, hi + 1)) for lo, hi in zip(BATCH["nmin"], BATCH["nmax"]))
+        out.append(dict(
+            nx=nx, ny=ny, nz=nz, layered=bool(rng.random() < 0.5), mseed=int(rng.integers(1 << 30)),
+            vp=float(rng.uniform(4000.0, 7000.0)), vpvs=float(rng.uniform(1.6, 1.9)), rho=float(rng.uniform(2200.0, 3000.0)),
+            src=(float(rng.uniform(pml + 1, nx - pml - 1) * d), float(rng.uniform(pml + 1, ny - pml - 1) * d),
+                 float(rng.uniform(1.0, nz - pml - 1) * d)),
+            f0=float(rng.uniform(*BATCH["f0"])), steps=int(rng.integers(BATCH["steps"][0], BATCH["steps"][1] + 1))))
+    return out
+
+
+def build_batch_model(sp):
+    from gfb import mesh
+
+    d, pml = BATCH["d"], BATCH["pml"]
+    faces = {"xmin": pml, "xmax": pml, "ymin": pml, "ymax": pml, "zmax": pml}
+    spec = mesh.MeshSpec(nx=sp["nx"], ny=sp["ny"], nz=sp["nz"], dx=d, dy=d, dz=d, order=4, pml=faces)
+    mat = (mesh.seeded_layers(sp["mseed"], sp["nz"] * d) if sp["layered"]
+           else mesh.homogeneous(sp["vp"], sp["vp"] / sp["vpvs"], sp["rho"]))
+    p = mesh.build_problem(spec, mat, np.array(sp["src"]), nsteps=sp["steps"], snapshot_stride=BATCH["stride"],
+                           record_depth_max_m=d, f0=sp["f0"])
+    for k in ("coords", "vp", "vs"):  # not solver inputs
+        p.pop(k, None)
+    return p
+
+
+def build_batch(threads: int = 8):
+    from concurrent.futures import ThreadPoolExecutor
+
+    specs = batch_specs()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        probs = list(ex.map(build_batch_model, specs))
+    return specs, probs
+
+
+def run_batch(args):
+    """32 models of uneven size in one solver: one element launch per colour
+    over all of them, the step replayed as a CUDA graph, kernel variant picked
+    by the autotuner.  Reported: aggregate GLL-point updates/s over the whole
+    run (every model to its last step) and each model's completion time."""
+    import gfb
+
+    t0 = time.perf_counter()
+    specs, probs = build_batch()
+    t_gen = time.perf_counter() - t0
+    dirs = [0, 1, 2][: args.fields]
+    n_steps = [sp["steps"] for sp in specs]
+    flags = gfb.FLAG_RECORD_F32 | gfb.FLAG_AUTOTUNE
+    t0 = time.perf_counter()
+    b = gfb.BatchSolver(probs, dirs=dirs, precision=gfb.FP32, device=args.device, record_slots=8, flags=flags,
+                        n_steps=n_steps)
+    t_create = time.perf_counter() - t0
+    info = b.info()
+    consumer = RecordConsumer(b)
+    order = sorted(set(n_steps))
+    finish, done, dev_ms = {}, 0, 0.0
+    with ClockSampler(args.device) as clk:
+        consumer.start()
+        for target in order:
+            dev_ms += b.advance_timed(target - done)
+            done = target
+            finish[target] = dev_ms
+        consumer.stop()
+    launches = b.info()["kernel_launches"]
+    b.drain()
+    b.close()
+    units = sum(p["n_cell"] * 125 * len(dirs) * n for p, n in zip(probs, n_steps))
+    value = units / (dev_ms / 1e3)
+    per_model = [{"cells": p["n_cell"], "steps": n, "finish_ms": finish[n],
+                  "gll_pt_updates": p["n_cell"] * 125 * len(dirs) * n} for p, n in zip(probs, n_steps)]
+    line = {
+        "metric": "aggregate GLL-point updates/s, 32 uneven models batched (FP32 x/y/z, 1 B200)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": max(n_steps), "warmup": 0,
+        "ms_per_step": dev_ms / max(n_steps), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batch32", "n_model": len(probs), "cells_total": int(sum(p["n_cell"] for p in probs)),
+                   "fields": len(dirs), "seed": BATCH["seed"], "generation_s": t_gen, "create_s": t_create,
+                   "elem_kernel": "line" if info["elem_kernel"] else "point",
+                   "cells_per_group": info["cells_per_group"], "elem_blocks": info["elem_blocks"],
+                   "graph": True, "l2": "inputs larger than L2"},
+        "per_model": per_model,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def max_over_ranks(seconds: float, dist, device: str) -> float:
@@ -423,6 +521,7 @@ def run_gfb(args):
                    "fields": len(dirs), "precision": args.precision, "state": "f64 u,v",
                    "l2": "inputs larger than L2 (geometry alone > 700 MB)", "parallelism": f"replicas{world}",
                    "n_colour": info["n_colour"], "n_pml_cell": info["n_pml_cell"],
+                   "elem_blocks": info["elem_blocks"],
                    "snapshots": f"every {prob['snapshot_stride']} steps, {info['n_rec_cell']} surface cells, "
                                 f"{'float32' if args.record_f32 else 'float64'}, copied to pinned host memory during the step "
                                 f"loop and released by a reader thread"},
@@ -458,7 +557,7 @@ def main():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gfb", choices=["gfb", "reference"])
-    ap.add_argument("--workload", default="layered_64x64x32", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="layered_64x64x32", choices=sorted(WORKLOADS) + ["batch32"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
@@ -473,6 +572,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch32":
+        return run_batch(args)
     return run_gfb(args)
 
 

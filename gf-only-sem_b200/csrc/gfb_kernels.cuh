@@ -45,6 +45,19 @@ __device__ __forceinline__ long long padded_index(long long g, int f, int F) {
     return g * (F / 3) * 4 + (f / 3) * 4 + (f % 3);
 }
 
+// Node-table rows used by the pipelined kernels: the NN node words of a
+// cell, then the index of the model the cell belongs to, padded to whole
+// 16-byte copies.
+__host__ __device__ constexpr int ib_row_words(int nn) { return (nn + 1 + 3) / 4 * 4; }
+
+// Time-step constants of one model (several independent models can share
+// one solver): dt, dt^2/2 (beta = 0) and the C-PML field coefficients
+// c1 = (1-2 theta) dt/2, c2 = (1-theta) dt^2/2 of pml.cpp:35, 63-64.
+struct ModelConst {
+    double dt, half_dt2, c1, c2;
+};
+constexpr int kMaxModels = 255;
+
 template <int NG>
 struct Shape {
     static constexpr int NN = NG * NG * NG;
@@ -65,6 +78,10 @@ struct NodeArgs {
     const Real* inv_mass;   // [n_node] 1/m (FP32 path) or nullptr
     const double* damping;  // [n_node] or nullptr
     double dt, half_dt2, beta, gamma;
+    // several models: model of each node, its constants, whether it still steps
+    const uint8_t* node_model;
+    const ModelConst* mc;
+    const int* mlive;
 };
 
 // C-PML at global nodes (FP32 path).
@@ -80,12 +97,14 @@ struct NodeArgs {
 // term is B1 v + B2 u + B3 m_x + B4 m_y + B5 m_z with B_k = sum over the
 // node's C-PML cells of w J/rho A_k.  The host checks the axis coefficients
 // agree across cells before choosing this form.
+// The C-PML nodes are the device nodes [0, n_slot): a node's slot is its
+// index.
 template <typename Real>
 struct NodePml {
-    const int* slot;     // [n_node] -1 or C-PML node slot
     const Real* coef;    // [slot][14]: B1..B5, alpha x(3), y(3), z(3)
-    Real* mem;           // [slot][F][3]
+    Real* mem;           // [axis][slot][F]; only live axes are read or written
     Real* prev;          // [slot][F]  last step's u + c1 v
+    long long n_slot;
     double c1, c2;
 };
 
@@ -111,7 +130,9 @@ struct ElemArgs {
     const int* src_head;  // [cell] first source slot or -1
     const int* src_next;  // [slot]
     const Real* src_w;    // [slot][NN]
-    Real stf;
+    const Real* mstf;     // [model] source time function value of this step (nullptr: none)
+    const int* mlive;     // [model] 1 while the model still steps
+    const ModelConst* mc; // [model]
     int dir0, dir1, dir2;
     // finalisation of the nodes whose last touching colour this is (the
     // node update fused into the element kernel); fuse == 0 keeps the
@@ -256,12 +277,13 @@ __device__ __forceinline__ void elem_body(const ElemArgs<Real>& A, Real* smem) {
         }
     }
     // point-force source
-    if (A.stf != Real(0)) {
+    const Real stf = A.mstf ? A.mstf[0] : Real(0);
+    if (stf != Real(0)) {
         int s = A.src_head ? __ldg(A.src_head + e) : -1;
         while (s >= 0) {
             const Real w = __ldg(A.src_w + (size_t)s * NN + p);
             if (w != Real(0)) {
-                const Real sw = A.stf * w;
+                const Real sw = stf * w;
                 const int dirs[3] = {A.dir0, A.dir1, A.dir2};
 #pragma unroll
                 for (int d = 0; d < NFLD; ++d)
@@ -323,52 +345,74 @@ __device__ __forceinline__ void store4(double* p, double a, double b, double c, 
 // Finalise wavefield d of node g from its complete assembled force fv:
 // node C-PML term (when PML), Newmark corrector with the diagonal mass
 // (solver.cpp:52-69, legacy damping of 564-574 applied to v first) and the
-// next step's predictor (40-49), written as one 16-byte vector.
+// next step's predictor (40-49), written as one 16-byte vector.  Every load
+// is issued before the first store, so a thread's memory round trips
+// overlap.  On the FP32 path 1/m == 0 marks a node with m <= 0 (the host
+// stores 0 there), so the f64 mass is not read.
 template <typename Real, int NFLD, bool PML>
 __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const NodePml<Real>& P, long long g,
-                                                  int d, const Real (&fv)[3]) {
+                                                  int d, const Real (&fv)[3], int sl, const ModelConst& K) {
     constexpr int F = 3 * NFLD;
-    const double m = A.mass[g];
-    const double dmp = A.damping ? A.damping[g] : 0.0;
-    const Real im = A.inv_mass ? A.inv_mass[g] : Real(0);
-    int sl = -1;
-    if (PML) sl = __ldg(P.slot + g);
+    const long long i0 = g * F + d * 3;
+    double* __restrict__ pu = A.u + i0;
+    double* __restrict__ pv = A.v + i0;
+    Real* __restrict__ pa = A.a + i0;
+    double vv[3], uu[3];
+    Real ao[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        vv[c] = pv[c];
+        uu[c] = pu[c];
+        ao[c] = pa[c];
+    }
+    const Real im = A.inv_mass ? __ldg(A.inv_mass + g) : Real(0);
+    const bool massless = A.inv_mass ? (im == Real(0)) : (__ldg(A.mass + g) <= 0.0);
+    const double m = A.inv_mass ? 1.0 : __ldg(A.mass + g);
+    const double dmp = A.damping ? __ldg(A.damping + g) : 0.0;
+    Real cf[14], mm[3][3], pr[3];
+    if (PML) {
+        if (sl >= 0) {
+#pragma unroll
+            for (int q = 0; q < 14; ++q) cf[q] = __ldg(P.coef + (size_t)sl * 14 + q);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    mm[q][c] = cf[2 + q] != Real(0) ? P.mem[((size_t)q * P.n_slot + sl) * F + d * 3 + c] : Real(0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pr[c] = P.prev[(size_t)sl * F + d * 3 + c];
+        }
+    }
     Real out[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const int f = d * 3 + c;
-        const long long idx = g * F + f;
-        double vv = A.v[idx];
-        if (dmp > 0.0) vv -= dmp * vv;
-        double uu = A.u[idx];
-        const double a_old = (double)A.a[idx];
+        if (dmp > 0.0) vv[c] -= dmp * vv[c];
         Real force = fv[c];
         if (PML && sl >= 0) {
-            const Real* cf = P.coef + (size_t)sl * 14;
-            Real* mm = P.mem + ((size_t)sl * F + f) * 3;
-            Real* pv = P.prev + (size_t)sl * F + f;
-            const Real nv = (Real)(uu + P.c1 * vv);
-            const Real ov = *pv + (Real)P.c2 * (Real)a_old;
-            const Real m0 = mm[0], m1 = mm[1], m2 = mm[2];
-            force += cf[0] * (Real)vv + cf[1] * (Real)uu + cf[2] * m0 + cf[3] * m1 + cf[4] * m2;
-            if (cf[2] != Real(0)) mm[0] = cf[5] * m0 + cf[6] * nv + cf[7] * ov;
-            if (cf[3] != Real(0)) mm[1] = cf[8] * m1 + cf[9] * nv + cf[10] * ov;
-            if (cf[4] != Real(0)) mm[2] = cf[11] * m2 + cf[12] * nv + cf[13] * ov;
-            *pv = nv;
+            const Real nv = (Real)(uu[c] + K.c1 * vv[c]);
+            const Real ov = pr[c] + (Real)K.c2 * ao[c];
+            force += cf[0] * (Real)vv[c] + cf[1] * (Real)uu[c] + cf[2] * mm[0][c] + cf[3] * mm[1][c] + cf[4] * mm[2][c];
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (cf[2 + q] != Real(0))
+                    P.mem[((size_t)q * P.n_slot + sl) * F + d * 3 + c] =
+                        cf[5 + 3 * q] * mm[q][c] + cf[6 + 3 * q] * nv + cf[7 + 3 * q] * ov;
+            P.prev[(size_t)sl * F + d * 3 + c] = nv;
         }
         double a_new;
-        if (m <= 0.0) {
+        if (massless) {
             a_new = 0.0;
         } else {
             a_new = A.inv_mass ? (double)(force * im) : (double)force / m;
             a_new = (double)(Real)a_new;
-            uu += A.dt * vv + A.dt * A.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
-            vv += A.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
+            const double a_old = (double)ao[c];
+            uu[c] += K.dt * vv[c] + K.dt * K.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
+            vv[c] += K.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
         }
-        A.u[idx] = uu;
-        A.v[idx] = vv;
-        A.a[idx] = (Real)a_new;
-        out[c] = (Real)(uu + A.dt * vv + A.half_dt2 * a_new);
+        pu[c] = uu[c];
+        pv[c] = vv[c];
+        pa[c] = (Real)a_new;
+        out[c] = (Real)(uu[c] + K.dt * vv[c] + K.half_dt2 * a_new);
     }
     store4(A.ut + ((size_t)g * NFLD + d) * 4, out[0], out[1], out[2], Real(0));
 }
@@ -376,19 +420,73 @@ __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const
 // Separate node pass (used when the element kernel does not finalise nodes):
 // one thread per (node, wavefield), the wavefields of a node in adjacent
 // threads, so a warp streams contiguous u, v, a and force/prediction
-// vectors and reads each node's mass / C-PML slot once.
-template <typename Real, int NFLD, bool PML>
-__global__ void node_update_kernel(NodeArgs<Real> A, NodePml<Real> P) {
-    const long long total = A.n_node * NFLD;
+// vectors and reads each node's mass once.  With node-form C-PML the pass
+// is two launches over contiguous node ranges: node_update_kernel over the
+// plain nodes [g0, n_node) without the C-PML registers, node_pml_kernel
+// over the C-PML nodes [0, g0).
+// Constants of the model node g belongs to; false when that model has
+// taken all its steps (its state stays as it is).
+template <typename Real, bool MULTI>
+__device__ __forceinline__ bool node_constants(const NodeArgs<Real>& A, const NodePml<Real>& P, long long g,
+                                               ModelConst& K) {
+    if (!MULTI) {
+        K = ModelConst{A.dt, A.half_dt2, P.c1, P.c2};
+        return true;
+    }
+    const int m = __ldg(A.node_model + g);
+    if (!__ldg(A.mlive + m)) return false;
+    K = A.mc[m];
+    return true;
+}
+
+template <typename Real, int NFLD, bool MULTI>
+__global__ void __launch_bounds__(256, 3) node_update_kernel(NodeArgs<Real> A, NodePml<Real> P, long long g0) {
+    const long long total = (A.n_node - g0) * NFLD;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const long long gl = t / NFLD;
+        const int d = (int)(t - gl * NFLD);
+        const long long g = g0 + gl;
+        ModelConst K;
+        if (!node_constants<Real, MULTI>(A, P, g, K)) continue;
+        Real fv4[4];
+        load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv4);
+        const Real fv[3] = {fv4[0], fv4[1], fv4[2]};
+        update_node_field<Real, NFLD, false>(A, P, g, d, fv, -1, K);
+    }
+}
+
+template <typename Real, int NFLD, bool MULTI>
+__global__ void __launch_bounds__(256, 2) node_pml_kernel(NodeArgs<Real> A, NodePml<Real> P) {
+    const long long total = P.n_slot * NFLD;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
         const long long g = t / NFLD;
         const int d = (int)(t - g * NFLD);
+        ModelConst K;
+        if (!node_constants<Real, MULTI>(A, P, g, K)) continue;
         Real fv4[4];
         load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv4);
         const Real fv[3] = {fv4[0], fv4[1], fv4[2]};
-        update_node_field<Real, NFLD, PML>(A, P, g, d, fv);
+        update_node_field<Real, NFLD, true>(A, P, g, d, fv, (int)g, K);
     }
+}
+
+// Start of a step for every model: whether it still steps, and its source
+// time function value (solver.cpp:577-605 uses stf_values[step]; steps past
+// the end of the series inject nothing).  mstep[m] is the step about to be
+// computed and moves on by one while the model steps, so a captured step
+// replays correctly.
+template <typename Real>
+__global__ void step_begin_kernel(int n_model, int* mstep, const int* nsteps, const int* n_stf,
+                                  const long long* stf_off, const Real* stf_all, Real* mstf, int* mlive) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_model) return;
+    const int t = mstep[m];
+    const bool live = t < nsteps[m];
+    mlive[m] = live ? 1 : 0;
+    mstf[m] = (live && t < n_stf[m]) ? stf_all[stf_off[m] + t] : Real(0);
+    mstep[m] = t + (live ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -400,8 +498,8 @@ __global__ void node_update_kernel(NodeArgs<Real> A, NodePml<Real> P) {
 // stages (3 stages for geometry/ibool, 2 for the gathered vectors), so each
 // SM keeps tens of KB of loads outstanding independent of how many blocks
 // fit.  Thread per GLL point; the n_field wavefields are looped per thread.
-// Node table on the device is padded to NNP entries per cell so every copy
-// is a 16-byte cp.async.
+// Node table rows on the device hold the cell's model index after its node
+// words and are padded so every copy is a 16-byte cp.async.
 // ---------------------------------------------------------------------------
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -418,7 +516,7 @@ struct PipeShape {
     static constexpr int EPB = NNP <= 32 ? 8 : (NNP <= 64 ? 4 : (NNP <= 128 ? 2 : 1));
     static constexpr int THREADS = NNP * EPB;
     static constexpr int GEO_B = 12 * NN * (int)sizeof(Real);         // geometry bytes per cell
-    static constexpr int IB_B = NNP * 4;                               // node-table bytes per cell
+    static constexpr int IB_B = ib_row_words(NN) * 4;                  // node-table bytes per cell
     static constexpr int BUF_B = NN * NFLD * 4 * (int)sizeof(Real);    // field vectors per cell
     // a geometry stage also receives the cell's old force vectors once the
     // geometry has been read into registers
@@ -510,7 +608,8 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
         cp_async_wait_all();
         __syncthreads();  // vectors + geometry of this group, node table of the next
         const int e = A.e_begin + grp * EPB + el;
-        const bool active = (e < A.e_end) && (p < NN);
+        const int mdl = (e < A.e_end) ? (int)ib_of(ist, el)[NN] : 0;
+        const bool active = (e < A.e_end) && (p < NN) && (!A.mlive || __ldg(A.mlive + mdl));
         Real* geo = geo_of(cur, el);
         Real* buf = buf_of(cur, el);
         uint32_t gword = 0;
@@ -620,6 +719,7 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
             // C-PML per cell (pml.cpp:55-216)
             const int slot = A.pml_slot ? __ldg(A.pml_slot + e) : -1;
             if (slot >= 0) {
+                const double c1 = A.mc ? A.mc[mdl].c1 : A.c1, c2 = A.mc ? A.mc[mdl].c2 : A.c2;
                 const Real* cf = A.pml_coef + (size_t)slot * 15 * NN + p;
                 Real al[9], ab[5];
 #pragma unroll
@@ -637,8 +737,8 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
                         const double un = A.u[(size_t)g * 3 * NFLD + f];
                         const double vn = A.v[(size_t)g * 3 * NFLD + f];
                         const Real an = A.a[(size_t)g * 3 * NFLD + f];
-                        const Real nv = Real(un + A.c1 * vn);
-                        const Real ov = prev[f * NN] + Real(A.c2) * an;
+                        const Real nv = Real(un + c1 * vn);
+                        const Real ov = prev[f * NN] + Real(c2) * an;
                         Real m0 = mem[(f * 3 + 0) * NN], m1 = mem[(f * 3 + 1) * NN], m2 = mem[(f * 3 + 2) * NN];
                         r[d][c] += scale * (ab[0] * Real(vn) + ab[1] * Real(un) + ab[2] * m0 + ab[3] * m1 + ab[4] * m2);
                         mem[(f * 3 + 0) * NN] = al[0] * m0 + al[1] * nv + al[2] * ov;
@@ -649,12 +749,13 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
                 }
             }
             // point force (solver.cpp:577-605)
-            if (A.stf != Real(0)) {
+            const Real stf = A.mstf ? __ldg(A.mstf + mdl) : Real(0);
+            if (stf != Real(0)) {
                 int s = A.src_head ? __ldg(A.src_head + e) : -1;
                 while (s >= 0) {
                     const Real w = __ldg(A.src_w + (size_t)s * NN + p);
                     if (w != Real(0)) {
-                        const Real sw = A.stf * w;
+                        const Real sw = stf * w;
 #pragma unroll
                         for (int d = 0; d < NFLD; ++d) {
                             const int dir = (d == 0) ? A.dir0 : ((d == 1) ? A.dir1 : A.dir2);
@@ -681,8 +782,11 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
                 if (!first) load4(geo + (p * NFLD + d) * 4, fo);
                 if (fin) {
                     const Real fv[3] = {fo[0] + r[d][0], fo[1] + r[d][1], fo[2] + r[d][2]};
-                    if (A.np.slot) update_node_field<Real, NFLD, true>(A.nu, A.np, g, d, fv);
-                    else update_node_field<Real, NFLD, false>(A.nu, A.np, g, d, fv);
+                    const ModelConst K = A.mc ? A.mc[mdl] : ModelConst{A.nu.dt, A.nu.half_dt2, A.np.c1, A.np.c2};
+                    if (A.np.coef)
+                        update_node_field<Real, NFLD, true>(A.nu, A.np, g, d, fv, g < A.np.n_slot ? (int)g : -1, K);
+                    else
+                        update_node_field<Real, NFLD, false>(A.nu, A.np, g, d, fv, -1, K);
                 } else {
                     store4(A.force + ((size_t)g * NFLD + d) * 4, fo[0] + r[d][0], fo[1] + r[d][1], fo[2] + r[d][2],
                            Real(0));
@@ -712,16 +816,22 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
 //
 // Pipelining: the geometry of the next group and the node table of the one
 // after are cp.async copies into rotating shared stages; the next group's
-// predicted-displacement vectors and this group's old force vectors are
-// register loads issued a phase ahead of their use.
+// predicted-displacement vectors are register loads issued one group ahead,
+// this group's old force vectors register loads issued once its gradient
+// phase is done.
 // ---------------------------------------------------------------------------
 
-template <int NG, int NFLD>
+// Cells per group of the line kernel: about 150 threads by default; the
+// autotuner also tries the neighbouring counts at ngll 5.
+__host__ __device__ constexpr int col_default_epb(int ng, int nfld) {
+    return (150 / (nfld * ng * ng)) > 0 ? 150 / (nfld * ng * ng) : 1;
+}
+
+template <int NG, int NFLD, int EPB_ = col_default_epb(NG, NFLD)>
 struct ColShape {
     static constexpr int NN = NG * NG * NG;
     static constexpr int NG2 = NG * NG;
-    static constexpr int NNP = (NN + 31) / 32 * 32;
-    static constexpr int EPB = (150 / (NFLD * NG2)) > 0 ? 150 / (NFLD * NG2) : 1;  // cells per group
+    static constexpr int EPB = EPB_;                      // cells per group
     static constexpr int GR = EPB * NFLD;                 // (cell, wavefield) lines per group
     static constexpr int ACTIVE = GR * NG2;               // threads with work
     static constexpr int THREADS = (ACTIVE + 31) / 32 * 32;
@@ -729,7 +839,7 @@ struct ColShape {
     static constexpr int GEO_B = 12 * NN * 4;
     static constexpr int GEO_W = GEO_B / 4;
     static constexpr int GEO_SLOT = GEO_B + 4 * (((24 - GEO_W) % 32 + 32) % 32 / 4 * 4);
-    static constexpr int IB_B = NNP * 4;
+    static constexpr int IB_B = ib_row_words(NN) * 4;
     static constexpr int ARR = 3 * GR * SP;               // floats of one [3][GR][SP] array
     static constexpr int SMEM = 2 * EPB * GEO_SLOT + 3 * EPB * IB_B + (3 * ARR + 64) * 4;
     static_assert(GEO_B % 16 == 0 && GEO_SLOT % 16 == 0 && IB_B % 16 == 0, "16-byte copies");
@@ -737,7 +847,7 @@ struct ColShape {
 
 struct ColArgs {
     int e_begin, e_end, n_groups;
-    const uint32_t* ibool_padded;  // [cell][NNP]
+    const uint32_t* ibool_padded;  // [cell][ib_row_words(NN)]: node words, model index
     const float* geom;             // [cell][12][NN]
     const float* ut;               // [node][NFLD][4]
     float* force;                  // [node][NFLD][4]
@@ -745,14 +855,17 @@ struct ColArgs {
     const int* src_head;
     const int* src_next;
     const float* src_w;
-    float stf;
+    const float* mstf;             // [model] source time function value of this step
+    const int* mlive;              // [model] 1 while the model still steps
+    int n_model;                   // <= kMaxModels
     int dir[3];
     float D[36];                   // D[i*NG+s], read with compile-time indices only
 };
 
-template <int NG, int NFLD>
-__global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kernel(ColArgs A) {
-    using S = ColShape<NG, NFLD>;
+template <int NG, int NFLD, int EPB_>
+__global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<NG, NFLD, EPB_>::THREADS <= 160 ? 3 : 2))
+    elem_col_kernel(ColArgs A) {
+    using S = ColShape<NG, NFLD, EPB_>;
     constexpr int NN = S::NN, NG2 = S::NG2, EPB = S::EPB, GR = S::GR, SP = S::SP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* gbase = smem_raw;
@@ -769,6 +882,13 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kerne
     const int cl = line / NFLD, fld = line - cl * NFLD;
     const int j = col / NG, k = col - j * NG;
     const int dir = fld == 0 ? A.dir[0] : (fld == 1 ? A.dir[1] : A.dir[2]);
+    // per-model step flags and source values of this step, read once per block
+    __shared__ float s_stf[kMaxModels];
+    __shared__ int s_live[kMaxModels];
+    for (int m = tid; m < A.n_model; m += S::THREADS) {
+        s_stf[m] = A.mstf[m];
+        s_live[m] = A.mlive[m];
+    }
     if (tid < NG2) sD[tid] = A.dmat[tid];
     __syncthreads();
     float Dj[NG], Dk[NG], Tj[NG], Tk[NG];
@@ -840,8 +960,9 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kerne
 
     int it = 0;
     for (int grp = grp0; grp < A.n_groups; grp += G, ++it) {
-        const bool act = pre_ok;
         const int e = A.e_begin + grp * EPB + cl;
+        const int mdl = pre_ok ? (int)ib_of(it % 3, cl)[NN] : 0;
+        const bool act = pre_ok && s_live[mdl];
         uint32_t cw[NG];
         float u0[NG], u1[NG], u2[NG];
 #pragma unroll
@@ -862,6 +983,8 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kerne
         if (nx < A.n_groups) issue_geo(nx, (it + 1) & 1);
         if (nx + G < A.n_groups) issue_ib(nx + G, (it + 2) % 3);
         cp_async_commit();
+        const float stf = act ? s_stf[mdl] : 0.f;
+        const int src = (act && stf != 0.f && A.src_head) ? __ldg(A.src_head + e) : -1;
         pre_ok = line_nodes(nx, (it + 1) % 3, nw);
         load_vectors(nw, pre_ok, pre);
 
@@ -932,7 +1055,6 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kerne
                         : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();  // fluxes of the whole group
         if (act) {
-            int src = (A.stf != 0.f && A.src_head) ? __ldg(A.src_head + e) : -1;
 #pragma unroll
             for (int i = 0; i < NG; ++i) {
                 const int p = i * NG2 + col;
@@ -961,7 +1083,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kerne
                 for (int sl = src; sl >= 0; sl = __ldg(A.src_next + sl)) {
                     const float w = __ldg(A.src_w + (size_t)sl * NN + p);
                     if (w != 0.f) {
-                        const float sw = A.stf * w;
+                        const float sw = stf * w;
                         if (dir == 0) r[0] += sw;
                         else if (dir == 1) r[1] += sw;
                         else r[2] += sw;
@@ -978,13 +1100,20 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD>::THREADS, 3) elem_col_kerne
 // Predictor only (start of a run or after a state overwrite).
 template <typename Real>
 __global__ void predict_kernel(long long n_node, int F, const double* u, const double* v, const Real* a,
-                               Real* ut, double dt, double half_dt2) {
+                               Real* ut, double dt, double half_dt2, const uint8_t* node_model,
+                               const ModelConst* mc) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long total = n_node * F;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
         const long long g = idx / F;
         const int f = (int)(idx - g * F);
-        ut[padded_index(g, f, F)] = (Real)(u[idx] + dt * v[idx] + half_dt2 * (double)a[idx]);
+        double h = dt, h2 = half_dt2;
+        if (node_model) {
+            const ModelConst& K = mc[node_model[g]];
+            h = K.dt;
+            h2 = K.half_dt2;
+        }
+        ut[padded_index(g, f, F)] = (Real)(u[idx] + h * v[idx] + h2 * (double)a[idx]);
         if (f % 3 == 2) ut[padded_index(g, f, F) + 1] = Real(0);
     }
 }

@@ -128,7 +128,7 @@ gfb_status run(int n_elem, const double* dxi_dx, const double* jacobian, const d
     A.dmat = dmat;
     A.pml_slot = nullptr;
     A.src_head = nullptr;
-    A.stf = 0.0;
+    A.mstf = nullptr;  // no source
     const int eblocks = (n_elem + S::EPB - 1) / S::EPB;
     gfb::elem_step_kernel<double, NG, 1>
         <<<eblocks, S::THREADS, gfb::elem_smem_bytes<double, NG, 1>(), stream>>>(A);

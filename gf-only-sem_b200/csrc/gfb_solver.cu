@@ -140,7 +140,6 @@ struct gfb_solver {
     bool fuse = false;  // node update in the element kernel's last colour
     int step = 0;
     std::vector<int> colour_begin;  // [n_colour+1] device cell ranges
-    std::vector<double> stf;
     bool has_cpml = false, has_damping = false, has_src = false;
     int n_pml = 0, n_src = 0, n_rec = 0, slots = 0;
     double c1 = 0.0, c2 = 0.0;
@@ -150,6 +149,10 @@ struct gfb_solver {
     uint32_t* ibool_padded = nullptr;  // [cell][NNP] for the pipelined kernel
     int pipe_blocks = 0;               // persistent grid of the element kernel
     int col_blocks = 0;                // persistent grid of the line kernel (FP32)
+    int col_variant = 0;               // cells per group: 0 default, 1 fewer, 2 more
+    int n_col_variants = 1;
+    int col_epb = 0;                   // cells per group of the variant in use
+    bool point_kernel = false;         // thread-per-point element kernel on the FP32 path
     void* geom = nullptr;
     void* dmat = nullptr;
     float dmat_host[36] = {};          // D of the line kernel's parameters
@@ -163,6 +166,19 @@ struct gfb_solver {
     int *src_head = nullptr, *src_next = nullptr;
     void* src_w = nullptr;
     int* rec_cell = nullptr;
+    // models sharing the solver (one for gfb_create): constants, step
+    // counters and source time functions on the device, so that a step
+    // captured in a CUDA graph replays correctly
+    int n_model = 1;
+    std::vector<int> model_nsteps;
+    gfb::ModelConst* d_mc = nullptr;
+    uint8_t* d_node_model = nullptr;   // [node] (several models only)
+    int *d_mlive = nullptr, *d_mstep = nullptr, *d_nsteps = nullptr, *d_nstf = nullptr;
+    long long* d_stf_off = nullptr;
+    void *d_mstf = nullptr, *d_stf_all = nullptr;
+    bool use_graph = true;
+    cudaGraphExec_t gexec = nullptr;   // one step: step start, colours, node pass
+    long long graph_launches = 0;
     void* ring = nullptr;              // device snapshot ring [slots]
     std::vector<void*> pinned;         // pinned host copy of each slot
     bool rec_f32 = false;              // snapshot values stored as float
@@ -178,7 +194,7 @@ struct gfb_solver {
     // C-PML kept at global nodes (FP32 path)
     bool node_pml = false;
     int n_pml_node = 0;
-    int* npml_slot = nullptr;
+    std::vector<int> node_perm, node_inv;  // device node -> node and back (empty: identity)
     void *npml_coef = nullptr, *npml_mem = nullptr, *npml_prev = nullptr;
     long long device_bytes = 0, upload_bytes = 0, launches = 0;
 
@@ -196,6 +212,7 @@ struct gfb_solver {
         return GFB_OK;
     }
     ~gfb_solver() {
+        if (gexec) cudaGraphExecDestroy(gexec);
         for (auto e : rec_evt) cudaEventDestroy(e);
         for (auto e : copy_evt) cudaEventDestroy(e);
         for (auto p : pinned) cudaFreeHost(p);
@@ -255,19 +272,22 @@ void node_args(const gfb_solver* s, gfb::NodeArgs<Real>& A, gfb::NodePml<Real>& 
     A.beta = 0.0;
     A.gamma = 0.5;
     A.half_dt2 = 0.5 * s->dt * s->dt * (1.0 - 2.0 * A.beta);
+    A.node_model = s->d_node_model;
+    A.mc = s->d_mc;
+    A.mlive = s->d_mlive;
     P = gfb::NodePml<Real>{};
     if (s->node_pml) {
-        P.slot = s->npml_slot;
         P.coef = static_cast<const Real*>(s->npml_coef);
         P.mem = static_cast<Real*>(s->npml_mem);
         P.prev = static_cast<Real*>(s->npml_prev);
-        P.c1 = s->c1;
-        P.c2 = s->c2;
+        P.n_slot = s->n_pml_node;
     }
+    P.c1 = s->c1;
+    P.c2 = s->c2;
 }
 
 template <typename Real, int NG, int NFLD>
-gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
+gfb_status launch_elem_t(gfb_solver* s, int c) {
     using S = gfb::PipeShape<Real, NG, NFLD>;
     gfb::ElemArgs<Real> A;
     A.e_begin = s->colour_begin[c];
@@ -291,7 +311,9 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
     A.src_head = s->has_src ? s->src_head : nullptr;
     A.src_next = s->src_next;
     A.src_w = static_cast<const Real*>(s->src_w);
-    A.stf = stf;
+    A.mstf = static_cast<const Real*>(s->d_mstf);
+    A.mlive = s->d_mlive;
+    A.mc = s->d_mc;
     A.dir0 = s->dirs[0];
     A.dir1 = s->dirs[1];
     A.dir2 = s->dirs[2];
@@ -308,14 +330,14 @@ gfb_status launch_elem_t(gfb_solver* s, int c, Real stf) {
 
 // The FP32 path runs the line kernel unless per-cell C-PML, the fused node
 // update or GFB_FLAG_POINT_KERNEL asks for the thread-per-point kernel.
-bool use_col_kernel(const gfb_solver* s) {
-    return s->prec == GFB_FP32 && !(s->has_cpml && !s->node_pml) && !s->fuse &&
-           !(s->flags & GFB_FLAG_POINT_KERNEL);
+bool col_kernel_eligible(const gfb_solver* s) {
+    return s->prec == GFB_FP32 && !(s->has_cpml && !s->node_pml) && !s->fuse;
 }
+bool use_col_kernel(const gfb_solver* s) { return col_kernel_eligible(s) && !s->point_kernel; }
 
-template <int NG, int NFLD>
-gfb_status launch_col_t(gfb_solver* s, int c, float stf) {
-    using S = gfb::ColShape<NG, NFLD>;
+template <int NG, int NFLD, int EPB>
+gfb_status launch_col_e(gfb_solver* s, int c) {
+    using S = gfb::ColShape<NG, NFLD, EPB>;
     gfb::ColArgs A;
     A.e_begin = s->colour_begin[c];
     A.e_end = s->colour_begin[c + 1];
@@ -330,15 +352,75 @@ gfb_status launch_col_t(gfb_solver* s, int c, float stf) {
     A.src_head = s->has_src ? s->src_head : nullptr;
     A.src_next = s->src_next;
     A.src_w = static_cast<const float*>(s->src_w);
-    A.stf = stf;
+    A.mstf = static_cast<const float*>(s->d_mstf);
+    A.mlive = s->d_mlive;
+    A.n_model = s->n_model;
     for (int d = 0; d < 3; ++d) A.dir[d] = s->dirs[d];
     for (int q = 0; q < 36; ++q) A.D[q] = q < NG * NG ? s->dmat_host[q] : 0.f;
     const int blocks = std::max(1, std::min(A.n_groups, s->col_blocks));
-    gfb::elem_col_kernel<NG, NFLD><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
+    gfb::elem_col_kernel<NG, NFLD, EPB><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
 }
+
+// Cells-per-group candidates of the line kernel: the default, and at
+// ngll 5 one fewer ("LO") and one more ("HI") step.
+constexpr int col_epb_lo(int nfld) { return nfld == 3 ? 1 : (nfld == 2 ? 2 : 4); }
+constexpr int col_epb_hi(int nfld) { return nfld == 3 ? 3 : (nfld == 2 ? 4 : 8); }
+template <int NG, int NFLD>
+struct ColEpb {
+    static constexpr int D = gfb::col_default_epb(NG, NFLD);
+    static constexpr int N = NG == 5 ? 3 : 1;
+};
+
+template <int NG, int NFLD>
+gfb_status launch_col_t(gfb_solver* s, int c) {
+    using E = ColEpb<NG, NFLD>;
+    if constexpr (E::N > 1) {
+        if (s->col_variant == 1) return launch_col_e<NG, NFLD, col_epb_lo(NFLD)>(s, c);
+        if (s->col_variant == 2) return launch_col_e<NG, NFLD, col_epb_hi(NFLD)>(s, c);
+    }
+    return launch_col_e<NG, NFLD, E::D>(s, c);
+}
+
+// Persistent grid of the line kernel variant EPB: occupancy x SMs.
+template <int NG, int NFLD, int EPB>
+gfb_status col_grid(gfb_solver* s, int* blocks) {
+    using C = gfb::ColShape<NG, NFLD, EPB>;
+    CU(cudaFuncSetAttribute(gfb::elem_col_kernel<NG, NFLD, EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    int per_sm = 0, n_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gfb::elem_col_kernel<NG, NFLD, EPB>, C::THREADS, C::SMEM));
+    CU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->device));
+    if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "line element kernel does not fit on an SM");
+    *blocks = per_sm * n_sm;
+    return GFB_OK;
+}
+
+template <int NG, int NFLD>
+gfb_status col_grid_t(gfb_solver* s) {
+    using E = ColEpb<NG, NFLD>;
+    gfb_status st;
+    s->n_col_variants = E::N;
+    if constexpr (E::N > 1) {
+        if (s->col_variant == 1) {
+            s->col_epb = col_epb_lo(NFLD);
+            return col_grid<NG, NFLD, col_epb_lo(NFLD)>(s, &s->col_blocks);
+        }
+        if (s->col_variant == 2) {
+            s->col_epb = col_epb_hi(NFLD);
+            return col_grid<NG, NFLD, col_epb_hi(NFLD)>(s, &s->col_blocks);
+        }
+    }
+    if ((st = col_grid<NG, NFLD, E::D>(s, &s->col_blocks))) return st;
+    s->col_epb = E::D;
+    return GFB_OK;
+}
+
+template <typename Real, int NG, int NFLD>
+struct ColGridOp {
+    static gfb_status run(gfb_solver* s) { return col_grid_t<NG, NFLD>(s); }
+};
 
 template <typename Real, int NG, int NFLD>
 gfb_status set_smem_t(gfb_solver* s) {
@@ -351,14 +433,7 @@ gfb_status set_smem_t(gfb_solver* s) {
     CU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->device));
     if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "element kernel does not fit on an SM");
     s->pipe_blocks = per_sm * n_sm;
-    if constexpr (std::is_same<Real, float>::value) {
-        using C = gfb::ColShape<NG, NFLD>;
-        CU(cudaFuncSetAttribute(gfb::elem_col_kernel<NG, NFLD>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gfb::elem_col_kernel<NG, NFLD>, C::THREADS,
-                                                         C::SMEM));
-        if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "line element kernel does not fit on an SM");
-        s->col_blocks = per_sm * n_sm;
-    }
+    if constexpr (std::is_same<Real, float>::value) return col_grid_t<NG, NFLD>(s);
     return GFB_OK;
 }
 
@@ -403,10 +478,10 @@ gfb_status dispatch(int ng, int nfld, Args... args) {
 
 template <typename Real, int NG, int NFLD>
 struct ElemOp {
-    static gfb_status run(gfb_solver* s, int c, double stf) {
+    static gfb_status run(gfb_solver* s, int c) {
         if constexpr (std::is_same<Real, float>::value)
-            if (use_col_kernel(s)) return launch_col_t<NG, NFLD>(s, c, (float)stf);
-        return launch_elem_t<Real, NG, NFLD>(s, c, (Real)stf);
+            if (use_col_kernel(s)) return launch_col_t<NG, NFLD>(s, c);
+        return launch_elem_t<Real, NG, NFLD>(s, c);
     }
 };
 template <typename Real, int NG, int NFLD>
@@ -418,9 +493,63 @@ struct RecOp {
     static gfb_status run(gfb_solver* s, void* out) { return launch_record_t<Real, NG, NFLD>(s, out); }
 };
 
-gfb_status launch_elem(gfb_solver* s, int c, double stf) {
-    if (s->prec == GFB_FP64) return dispatch<double, ElemOp>(s->ng, s->nfld, s, c, stf);
-    return dispatch<float, ElemOp>(s->ng, s->nfld, s, c, stf);
+gfb_status launch_elem(gfb_solver* s, int c) {
+    if (s->prec == GFB_FP64) return dispatch<double, ElemOp>(s->ng, s->nfld, s, c);
+    return dispatch<float, ElemOp>(s->ng, s->nfld, s, c);
+}
+
+// Autotuner of the FP32 element phase: times full colour sweeps of every
+// element-kernel candidate on this mesh (the line kernel with each cells-per-
+// group count it is built with, and the thread-per-point kernel) and keeps
+// the fastest.  A full sweep only rewrites the assembled force from the
+// current predicted displacement (the first colour touching a node stores),
+// so tuning leaves the solver's state as it was.
+gfb_status autotune(gfb_solver* s) {
+    if (!col_kernel_eligible(s)) return GFB_OK;
+    const int n_colour = (int)s->colour_begin.size() - 1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    struct Cand {
+        bool point;
+        int variant;
+        float ms;
+    };
+    std::vector<Cand> cands;
+    for (int v = 0; v < s->n_col_variants; ++v) cands.push_back({false, v, 0.0f});
+    cands.push_back({true, 0, 0.0f});
+    gfb_status st = GFB_OK;
+    const long long l0 = s->launches;
+    for (auto& c : cands) {
+        s->point_kernel = c.point;
+        s->col_variant = c.variant;
+        if (!c.point && (st = dispatch<float, ColGridOp>(s->ng, s->nfld, s))) break;
+        auto sweep = [&]() -> gfb_status {
+            gfb_status r;
+            for (int k = 0; k < n_colour; ++k)
+                if ((r = launch_elem(s, k))) return r;
+            return GFB_OK;
+        };
+        if ((st = sweep())) break;  // warm-up
+        if (cudaEventRecord(e0, s->stream) != cudaSuccess) { st = fail(GFB_ERR_CUDA, "autotune event"); break; }
+        for (int rep = 0; rep < 3 && !st; ++rep) st = sweep();
+        if (st) break;
+        if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&c.ms, e0, e1) != cudaSuccess) {
+            st = fail(GFB_ERR_CUDA, "autotune timing failed");
+            break;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->launches = l0;
+    if (st) return st;
+    const Cand* best = &cands[0];
+    for (const auto& c : cands)
+        if (c.ms < best->ms) best = &c;
+    s->point_kernel = best->point;
+    s->col_variant = best->point ? 0 : best->variant;
+    return dispatch<float, ColGridOp>(s->ng, s->nfld, s);
 }
 
 gfb_status launch_record(gfb_solver* s, void* out) {
@@ -433,17 +562,31 @@ int grid_for(long long n, int threads) {
     return (int)std::max(1LL, std::min(b, 148LL * 32));
 }
 
-template <typename Real, int NFLD>
-gfb_status launch_node_f(gfb_solver* s) {
+template <typename Real, int NFLD, bool MULTI>
+gfb_status launch_node_m(gfb_solver* s) {
     gfb::NodeArgs<Real> A;
     gfb::NodePml<Real> P;
     node_args(s, A, P);
-    const int grid = grid_for((long long)s->n_node * NFLD, 256);
-    if (s->node_pml) gfb::node_update_kernel<Real, NFLD, true><<<grid, 256, 0, s->stream>>>(A, P);
-    else gfb::node_update_kernel<Real, NFLD, false><<<grid, 256, 0, s->stream>>>(A, P);
-    CU(cudaGetLastError());
-    s->launches++;
+    // node-form C-PML nodes are device nodes [0, n_pml_node)
+    const long long g0 = s->node_pml ? s->n_pml_node : 0;
+    if (g0 < s->n_node) {
+        const int grid = grid_for((long long)(s->n_node - g0) * NFLD, 256);
+        gfb::node_update_kernel<Real, NFLD, MULTI><<<grid, 256, 0, s->stream>>>(A, P, g0);
+        CU(cudaGetLastError());
+        s->launches++;
+    }
+    if (g0 > 0) {
+        const int gp = grid_for(g0 * NFLD, 256);
+        gfb::node_pml_kernel<Real, NFLD, MULTI><<<gp, 256, 0, s->stream>>>(A, P);
+        CU(cudaGetLastError());
+        s->launches++;
+    }
     return GFB_OK;
+}
+
+template <typename Real, int NFLD>
+gfb_status launch_node_f(gfb_solver* s) {
+    return s->n_model > 1 ? launch_node_m<Real, NFLD, true>(s) : launch_node_m<Real, NFLD, false>(s);
 }
 
 template <typename Real>
@@ -462,7 +605,8 @@ gfb_status launch_predict_t(gfb_solver* s) {
     const long long n = (long long)s->n_node * s->F;
     const double h = 0.5 * s->dt * s->dt * (1.0 - 2.0 * 0.0);
     gfb::predict_kernel<Real><<<grid_for(n, 256), 256, 0, s->stream>>>(
-        (long long)s->n_node, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h);
+        (long long)s->n_node, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h,
+        s->d_node_model, s->d_mc);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -502,28 +646,34 @@ gfb_status spill(gfb_solver* s, Snapshot& snap) {
 // C-PML at global nodes: B_k = sum over C-PML cells at the node of
 // w J/rho A_k (k = 1..5, accumulated in FP64 in cell order), and for each
 // axis the convolution coefficients of the cells where that axis acts.
-// Leaves s->node_pml false (per-cell form) if two cells disagree on an
-// axis's coefficients at a shared node.
-template <typename Real>
-gfb_status build_node_pml(gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w) {
+// Returns false (per-cell form) if two cells disagree on an axis's
+// coefficients at a shared node.  slot[g] numbers the C-PML nodes in
+// increasing node order; coef is [slot][14].
+bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w, std::vector<int>& slot,
+                   std::vector<double>& coef) {
     const int ng = s->ng, nn = s->nn;
-    std::vector<int> slot(s->n_node, -1);
-    std::vector<double> acc;
-    std::vector<unsigned char> have;
+    auto live = [&](long long q) {
+        const double* A = m->pml_coef_abar + q * 5;
+        return A[0] != 0.0 || A[1] != 0.0 || A[2] != 0.0 || A[3] != 0.0 || A[4] != 0.0;
+    };
+    slot.assign(s->n_node, -1);
+    for (long long e = 0; e < s->n_cell; ++e)
+        if (m->pml_region[e] != 0)
+            for (int p = 0; p < nn; ++p)
+                if (live(e * nn + p)) slot[m->ibool[e * nn + p]] = 0;
     int n = 0;
+    for (int g = 0; g < s->n_node; ++g)
+        if (slot[g] >= 0) slot[g] = n++;
+    coef.assign((size_t)n * 14, 0.0);
+    std::vector<unsigned char> have(n, 0);
     for (long long e = 0; e < s->n_cell; ++e) {
         if (m->pml_region[e] == 0) continue;
         for (int p = 0; p < nn; ++p) {
             const long long q = e * nn + p;
+            if (!live(q)) continue;
             const double* A = m->pml_coef_abar + q * 5;
-            if (A[0] == 0.0 && A[1] == 0.0 && A[2] == 0.0 && A[3] == 0.0 && A[4] == 0.0) continue;
-            const int g = m->ibool[q];
-            if (slot[g] < 0) {
-                slot[g] = n++;
-                acc.resize((size_t)n * 14, 0.0);
-                have.push_back(0);
-            }
-            double* c = &acc[(size_t)slot[g] * 14];
+            const int sl = slot[m->ibool[q]];
+            double* c = &coef[(size_t)sl * 14];
             const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
             const double wgll = w[ni] * w[nj] * w[nk];
             const double rho = m->density[q];
@@ -532,32 +682,35 @@ gfb_status build_node_pml(gfb_solver* s, const gfb_mesh* m, const std::vector<do
             const double* al = m->pml_coef_alpha + q * 9;
             for (int ax = 0; ax < 3; ++ax) {
                 if (A[2 + ax] == 0.0) continue;
-                unsigned char& hv = have[slot[g]];
-                if (!(hv & (1u << ax))) {
+                if (!(have[sl] & (1u << ax))) {
                     for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
-                    hv |= (unsigned char)(1u << ax);
+                    have[sl] |= (unsigned char)(1u << ax);
                 } else {
                     for (int t = 0; t < 3; ++t) {
                         const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
-                        if (std::abs(a0 - a1) > 1e-9 * std::max(std::abs(a0), std::abs(a1))) return GFB_OK;
+                        if (std::abs(a0 - a1) > 1e-9 * std::max(std::abs(a0), std::abs(a1))) return false;
                     }
                 }
             }
         }
     }
+    return true;
+}
+
+// Upload the node-form C-PML: the C-PML nodes are device nodes [0, n)
+// (slot = device node), coefficients [slot][14], memory [axis][slot][F]
+// and the previous field [slot][F], both zero.
+template <typename Real>
+gfb_status upload_node_pml(gfb_solver* s, const std::vector<double>& coef) {
     gfb_status st;
-    {
-        int* d = nullptr;
-        if ((st = s->alloc(&d, slot.size()))) return st;
-        if ((st = h2d(s, d, slot.data(), slot.size() * 4))) return st;
-        s->npml_slot = d;
-    }
-    std::vector<Real> coef(acc.size());
-    for (size_t i = 0; i < acc.size(); ++i) coef[i] = (Real)acc[i];
-    if ((st = upload(s, &s->npml_coef, coef))) return st;
+    const int n = (int)(coef.size() / 14);
+    std::vector<Real> cf(coef.size());
+    for (size_t i = 0; i < coef.size(); ++i) cf[i] = (Real)coef[i];
+    if (cf.empty()) cf.push_back(Real(0));
+    if ((st = upload(s, &s->npml_coef, cf))) return st;
     Real *mem = nullptr, *prev = nullptr;
-    if ((st = s->alloc(&mem, (size_t)n * s->F * 3))) return st;
-    if ((st = s->alloc(&prev, (size_t)n * s->F))) return st;
+    if ((st = s->alloc(&mem, (size_t)std::max(n, 1) * s->F * 3))) return st;
+    if ((st = s->alloc(&prev, (size_t)std::max(n, 1) * s->F))) return st;
     CU(cudaMemset(mem, 0, (size_t)std::max(n, 1) * s->F * 3 * sizeof(Real)));
     CU(cudaMemset(prev, 0, (size_t)std::max(n, 1) * s->F * sizeof(Real)));
     s->npml_mem = mem;
@@ -568,24 +721,59 @@ gfb_status build_node_pml(gfb_solver* s, const gfb_mesh* m, const std::vector<do
 }
 
 template <typename Real>
-gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
-                        const std::vector<int>& perm, const std::vector<int>& inv_perm,
+gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src, int n_model,
+                        const gfb_model* models, const std::vector<int>& perm, const std::vector<int>& inv_perm,
                         const std::vector<uint32_t>& ibool_dev, const std::vector<double>& node_mass,
                         const std::vector<double>& node_damp, const std::vector<double>& w,
                         const std::vector<double>& D) {
     const int ng = s->ng, nn = s->nn;
     const long long n_cell = s->n_cell;
     gfb_status st;
+    // C-PML at global nodes (FP32 path) when the cells agree at shared nodes;
+    // its nodes become device nodes [0, n_pml_node), the others follow, both
+    // in increasing node order
+    std::vector<int> pslot;
+    std::vector<double> pcoef;
+    const bool node_form = s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML) &&
+                           plan_node_pml(s, m, w, pslot, pcoef);
+    s->node_perm.clear();
+    s->node_inv.clear();
+    if (node_form) {
+        s->node_perm.reserve(s->n_node);
+        for (int g = 0; g < s->n_node; ++g)
+            if (pslot[g] >= 0) s->node_perm.push_back(g);
+        for (int g = 0; g < s->n_node; ++g)
+            if (pslot[g] < 0) s->node_perm.push_back(g);
+        s->node_inv.assign(s->n_node, 0);
+        for (int d = 0; d < s->n_node; ++d) s->node_inv[s->node_perm[d]] = d;
+    }
+    auto dev_node = [&](long long g) -> long long { return s->node_inv.empty() ? g : s->node_inv[g]; };
+    auto permuted = [&](const std::vector<double>& h) {
+        if (s->node_perm.empty()) return h;
+        std::vector<double> o(h.size());
+        for (size_t d = 0; d < o.size(); ++d) o[d] = h[s->node_perm[d]];
+        return o;
+    };
     // ibool
     {
+        std::vector<uint32_t> ibd(ibool_dev);
+        if (!s->node_inv.empty())
+            for (auto& x : ibd) x = (x & ~gfb::kNodeMask) | (uint32_t)s->node_inv[x & gfb::kNodeMask];
         uint32_t* d = nullptr;
-        if ((st = s->alloc(&d, ibool_dev.size()))) return st;
-        if ((st = h2d(s, d, ibool_dev.data(), ibool_dev.size() * 4))) return st;
+        if ((st = s->alloc(&d, ibd.size()))) return st;
+        if ((st = h2d(s, d, ibd.data(), ibd.size() * 4))) return st;
         s->ibool = d;
-        const int nnp = (nn + 31) / 32 * 32;
+        // rows of the pipelined kernels: node words, then the cell's model
+        const int nnp = gfb::ib_row_words(nn);
         std::vector<uint32_t> pad((size_t)n_cell * nnp, 0u);
-        for (long long e = 0; e < n_cell; ++e)
-            for (int p = 0; p < nn; ++p) pad[e * nnp + p] = ibool_dev[e * nn + p];
+        int mi = 0;
+        for (long long e = 0; e < n_cell; ++e) {
+            for (int p = 0; p < nn; ++p) pad[e * nnp + p] = ibd[e * nn + p];
+            const int orig = perm[e];
+            mi = 0;
+            while (orig >= models[mi].cell_end) ++mi;
+            pad[e * nnp + nn] = (uint32_t)mi;
+        }
         uint32_t* dp = nullptr;
         if ((st = s->alloc(&dp, pad.size()))) return st;
         if ((st = h2d(s, dp, pad.data(), pad.size() * 4))) return st;
@@ -635,27 +823,26 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     CU(cudaMemset(a, 0, nF * sizeof(Real)));
     CU(cudaMemset(ut, 0, nP * sizeof(Real)));
     CU(cudaMemset(force, 0, nP * sizeof(Real)));
+    const std::vector<double> mass_d = permuted(node_mass);
     {
         double* d = nullptr;
-        if ((st = s->alloc(&d, node_mass.size()))) return st;
-        if ((st = h2d(s, d, node_mass.data(), node_mass.size() * 8))) return st;
+        if ((st = s->alloc(&d, mass_d.size()))) return st;
+        if ((st = h2d(s, d, mass_d.data(), mass_d.size() * 8))) return st;
         s->mass = d;
     }
     if (s->prec == GFB_FP32) {
-        std::vector<Real> im(node_mass.size());
-        for (size_t g = 0; g < im.size(); ++g) im[g] = node_mass[g] > 0.0 ? (Real)(1.0 / node_mass[g]) : Real(0);
+        std::vector<Real> im(mass_d.size());
+        for (size_t g = 0; g < im.size(); ++g) im[g] = mass_d[g] > 0.0 ? (Real)(1.0 / mass_d[g]) : Real(0);
         if ((st = upload(s, &s->inv_mass, im))) return st;
     }
     if (s->has_damping) {
+        const std::vector<double> damp_d = permuted(node_damp);
         double* d = nullptr;
-        if ((st = s->alloc(&d, node_damp.size()))) return st;
-        if ((st = h2d(s, d, node_damp.data(), node_damp.size() * 8))) return st;
+        if ((st = s->alloc(&d, damp_d.size()))) return st;
+        if ((st = h2d(s, d, damp_d.data(), damp_d.size() * 8))) return st;
         s->damping = d;
     }
-    // C-PML at global nodes (FP32 path) when the cells agree at shared nodes
-    if (s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML)) {
-        if ((st = build_node_pml<Real>(s, m, w))) return st;
-    }
+    if (node_form && (st = upload_node_pml<Real>(s, pcoef))) return st;
     // C-PML per cell
     if (s->has_cpml && !s->node_pml) {
         std::vector<int> slot(n_cell, -1);
@@ -730,7 +917,46 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         s->src_head = dh;
         s->src_next = dn;
         if ((st = upload(s, &s->src_w, wts))) return st;
-        s->stf.assign(src->stf, src->stf + std::max(0, src->n_stf));
+    }
+    // models: constants, step counters, source time functions
+    {
+        std::vector<gfb::ModelConst> mc(n_model);
+        std::vector<int> nsteps(n_model), nstf(n_model), zero(n_model, 0), one(n_model, 1);
+        std::vector<long long> off(n_model);
+        std::vector<Real> stf_all, mstf(n_model, Real(0));
+        const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
+        for (int k = 0; k < n_model; ++k) {
+            const double dt = models[k].dt;
+            mc[k] = gfb::ModelConst{dt, 0.5 * dt * dt, (1.0 - 2.0 * theta) * 0.5 * dt, (1.0 - theta) * 0.5 * dt * dt};
+            nsteps[k] = models[k].n_steps;
+            nstf[k] = std::max(0, models[k].n_stf);
+            off[k] = (long long)stf_all.size();
+            for (int t = 0; t < nstf[k]; ++t) stf_all.push_back((Real)models[k].stf[t]);
+        }
+        s->model_nsteps = nsteps;
+        if (stf_all.empty()) stf_all.push_back(Real(0));
+        auto put_int = [&](int** d, const std::vector<int>& h) -> gfb_status {
+            gfb_status r;
+            if ((r = s->alloc(d, h.size()))) return r;
+            return h2d(s, *d, h.data(), h.size() * 4);
+        };
+        if ((st = s->alloc(&s->d_mc, mc.size()))) return st;
+        if ((st = h2d(s, s->d_mc, mc.data(), mc.size() * sizeof(gfb::ModelConst)))) return st;
+        if ((st = put_int(&s->d_nsteps, nsteps))) return st;
+        if ((st = put_int(&s->d_nstf, nstf))) return st;
+        if ((st = put_int(&s->d_mstep, zero))) return st;
+        if ((st = put_int(&s->d_mlive, one))) return st;
+        if ((st = s->alloc(&s->d_stf_off, off.size()))) return st;
+        if ((st = h2d(s, s->d_stf_off, off.data(), off.size() * 8))) return st;
+        if ((st = upload(s, &s->d_stf_all, stf_all))) return st;
+        if ((st = upload(s, &s->d_mstf, mstf))) return st;
+        if (n_model > 1) {
+            std::vector<uint8_t> nm(s->n_node, 0);
+            for (int k = 0; k < n_model; ++k)
+                for (int g = models[k].node_begin; g < models[k].node_end; ++g) nm[dev_node(g)] = (uint8_t)k;
+            if ((st = s->alloc(&s->d_node_model, nm.size()))) return st;
+            if ((st = h2d(s, s->d_node_model, nm.data(), nm.size()))) return st;
+        }
     }
     if (s->node_pml) {
         s->n_pml = 0;
@@ -787,20 +1013,69 @@ gfb_status validate(const gfb_mesh* m, const gfb_config* c) {
 }
 
 
-// One solver step: NC colour launches, node update, optional snapshot.
-// With ev != nullptr, events 0..3 bracket the three phases on the stream.
-gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
+template <typename Real>
+gfb_status launch_step_begin_t(gfb_solver* s) {
+    const int threads = 128;
+    const int blocks = (s->n_model + threads - 1) / threads;
+    gfb::step_begin_kernel<Real><<<blocks, threads, 0, s->stream>>>(
+        s->n_model, s->d_mstep, s->d_nsteps, s->d_nstf, s->d_stf_off, static_cast<const Real*>(s->d_stf_all),
+        static_cast<Real*>(s->d_mstf), s->d_mlive);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+// The device work of one step: step start, NC colour launches, node pass.
+// With ev != nullptr, events 0..2 bracket the element and node phases.
+gfb_status step_body(gfb_solver* s, cudaEvent_t* ev) {
     gfb_status st;
     const int n_colour = (int)s->colour_begin.size() - 1;
-    const int step = s->step;
-    const double stf = (s->has_src && step < (int)s->stf.size()) ? s->stf[step] : 0.0;
     if (ev) CU(cudaEventRecord(ev[0], s->stream));
+    st = s->prec == GFB_FP64 ? launch_step_begin_t<double>(s) : launch_step_begin_t<float>(s);
+    if (st) return st;
     for (int c = 0; c < n_colour; ++c)
-        if ((st = launch_elem(s, c, stf))) return st;
+        if ((st = launch_elem(s, c))) return st;
     if (ev) CU(cudaEventRecord(ev[1], s->stream));
     if (!s->fuse)
         if ((st = launch_node(s))) return st;
     if (ev) CU(cudaEventRecord(ev[2], s->stream));
+    return GFB_OK;
+}
+
+// Capture step_body once as a CUDA graph; every argument it launches with
+// (device pointers, colour ranges, grid sizes) is fixed for the solver's
+// lifetime, and the step-dependent values live on the device.
+gfb_status capture_step(gfb_solver* s) {
+    const long long l0 = s->launches;
+    CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    gfb_status st = step_body(s, nullptr);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(GFB_ERR_CUDA, "step capture failed: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&s->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(GFB_ERR_CUDA, "step graph instantiation failed: %s", cudaGetErrorString(ei));
+    s->graph_launches = s->launches - l0;
+    s->launches = l0;
+    return GFB_OK;
+}
+
+// One solver step: the device work (a graph launch, or eager launches when
+// phases are timed), then the snapshot when the step is a snapshot step.
+gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
+    gfb_status st;
+    const int step = s->step;
+    if (!ev && s->use_graph) {
+        if (!s->gexec && (st = capture_step(s))) return st;
+        CU(cudaGraphLaunch(s->gexec, s->stream));
+        s->launches += s->graph_launches;
+    } else if ((st = step_body(s, ev))) {
+        return st;
+    }
     if (s->stride > 0 && s->n_rec > 0 && step % s->stride == 0) {
         // round-robin slot; an unread snapshot still in it moves to pageable
         // memory first.  The record kernel waits (on the GPU) for the last
@@ -846,11 +1121,13 @@ int32_t gfb_abi_version(void) { return GFB_ABI_VERSION; }
 
 const char* gfb_last_error(void) { return g_err.c_str(); }
 
-gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, gfb_solver** out) {
-    if (!out) return fail(GFB_ERR_INVALID, "out is NULL");
-    *out = nullptr;
-    gfb_status st = validate(m, c);
-    if (st) return st;
+}  // extern "C"
+
+namespace {
+
+gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, int n_model,
+                       const gfb_model* models, gfb_solver** out) {
+    gfb_status st;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(GFB_ERR_NO_DEVICE, "no CUDA-capable GPU found");
@@ -873,6 +1150,9 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     s->flags = c->flags;
     s->rec_f32 = (c->flags & GFB_FLAG_RECORD_F32) != 0;
     s->fuse = (c->flags & GFB_FLAG_FUSED_NODE) != 0;
+    s->use_graph = !(c->flags & GFB_FLAG_NO_GRAPH);
+    s->point_kernel = (c->flags & GFB_FLAG_POINT_KERNEL) != 0;
+    s->n_model = n_model;
     s->n_rec = m->n_rec_cell;
     s->slots = std::max(1, c->record_slots);
     const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
@@ -954,16 +1234,69 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     if (!gll_tables(m->ngll - 1, x, w, D)) return fail(GFB_ERR_INVALID, "GLL table construction failed");
     if (s->prec == GFB_FP64) {
         if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
-        st = build_device<double>(s.get(), m, src, perm, inv_perm, ibool_dev, node_mass, node_damp, w, D);
+        st = build_device<double>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
+                                  w, D);
     } else {
         if ((st = dispatch<float, SmemOp>(s->ng, s->nfld, s.get()))) return st;
-        st = build_device<float>(s.get(), m, src, perm, inv_perm, ibool_dev, node_mass, node_damp, w, D);
+        st = build_device<float>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
+                                 w, D);
     }
     if (st) return st;
     CU(cudaStreamSynchronize(s->stream));
+    if ((c->flags & GFB_FLAG_AUTOTUNE) && (st = autotune(s.get()))) return st;
     CU(cudaDeviceSynchronize());
     *out = s.release();
     return GFB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, gfb_solver** out) {
+    if (!out) return fail(GFB_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    gfb_status st = validate(m, c);
+    if (st) return st;
+    gfb_model one{};
+    one.cell_begin = 0;
+    one.cell_end = m->n_cell;
+    one.node_begin = 0;
+    one.node_end = m->n_node;
+    one.dt = c->dt;
+    one.n_steps = INT32_MAX;
+    one.n_stf = src ? src->n_stf : 0;
+    one.stf = src ? src->stf : nullptr;
+    return create_impl(m, c, src, 1, &one, out);
+}
+
+gfb_status gfb_create_batch(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, int32_t n_model,
+                            const gfb_model* models, gfb_solver** out) {
+    if (!out) return fail(GFB_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!models || n_model < 1 || n_model > 255) return fail(GFB_ERR_INVALID, "n_model must be 1..255");
+    if (!m || !c) return fail(GFB_ERR_INVALID, "mesh and config are required");
+    gfb_config cc = *c;
+    cc.dt = models[0].dt;
+    gfb_status st = validate(m, &cc);
+    if (st) return st;
+    for (int k = 0; k < n_model; ++k) {
+        const gfb_model& md = models[k];
+        const int cb = k ? models[k - 1].cell_end : 0, nb = k ? models[k - 1].node_end : 0;
+        if (md.cell_begin != cb || md.cell_end <= md.cell_begin || md.node_begin != nb || md.node_end <= md.node_begin)
+            return fail(GFB_ERR_INVALID, "model %d: cells and nodes must follow the previous model's", k);
+        if (!(md.dt > 0.0)) return fail(GFB_ERR_INVALID, "model %d: dt must be positive", k);
+        if (md.n_steps < 0 || md.n_stf < 0 || (md.n_stf > 0 && !md.stf))
+            return fail(GFB_ERR_INVALID, "model %d: bad step count or source time function", k);
+    }
+    if (models[n_model - 1].cell_end != m->n_cell || models[n_model - 1].node_end != m->n_node)
+        return fail(GFB_ERR_INVALID, "models must cover all %d cells and %d nodes", m->n_cell, m->n_node);
+    const int nn = m->ngll * m->ngll * m->ngll;
+    for (int k = 0; k < n_model; ++k)
+        for (long long q = (long long)models[k].cell_begin * nn; q < (long long)models[k].cell_end * nn; ++q)
+            if (m->ibool[q] < models[k].node_begin || m->ibool[q] >= models[k].node_end)
+                return fail(GFB_ERR_INVALID, "model %d: cell %lld uses node %d of another model", k, q / nn, m->ibool[q]);
+    return create_impl(m, &cc, src, n_model, models, out);
 }
 
 gfb_status gfb_destroy(gfb_solver* s) {
@@ -983,6 +1316,29 @@ gfb_status gfb_advance(gfb_solver* s, int32_t n_steps) {
         if (st) return st;
     }
     return GFB_OK;
+}
+
+gfb_status gfb_advance_timed(gfb_solver* s, int32_t n_steps, double* ms) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (n_steps < 0) return fail(GFB_ERR_INVALID, "n_steps must be >= 0");
+    CU(cudaSetDevice(s->device));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(GFB_ERR_CUDA, "cudaEventCreate failed");
+    }
+    gfb_status st = GFB_OK;
+    if (cudaEventRecord(e0, s->stream) != cudaSuccess) st = fail(GFB_ERR_CUDA, "cudaEventRecord failed");
+    for (int it = 0; it < n_steps && !st; ++it) st = one_step(s, nullptr);
+    float t = 0.0f;
+    if (!st && (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+        st = fail(GFB_ERR_CUDA, "step timing failed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!st && ms) *ms += t;
+    return st;
 }
 
 gfb_status gfb_advance_profiled(gfb_solver* s, int32_t n_steps, double* ms_element, double* ms_node,
@@ -1036,7 +1392,9 @@ gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
     info->upload_bytes = s->upload_bytes;
     info->kernel_launches = s->launches;
     info->n_pml_node = s->node_pml ? s->n_pml_node : 0;
-    info->reserved = 0;
+    info->elem_blocks = use_col_kernel(s) ? s->col_blocks : s->pipe_blocks;
+    info->elem_kernel = use_col_kernel(s) ? 1 : 0;
+    info->cells_per_group = use_col_kernel(s) ? s->col_epb : 0;
     return GFB_OK;
 }
 
@@ -1061,9 +1419,11 @@ gfb_status gfb_get_state(gfb_solver* s, int32_t field, double* u, double* v, dou
     const size_t nF = (size_t)s->n_node * s->F;
     std::vector<double> tmp(nF);
     gfb_status st;
-    auto pick = [&](double* dst) {  // device layout [node][3*n_field]
-        for (long long g = 0; g < s->n_node; ++g)
-            for (int c = 0; c < 3; ++c) dst[g * 3 + c] = tmp[g * s->F + field * 3 + c];
+    auto pick = [&](double* dst) {  // device layout [device node][3*n_field]
+        for (long long g = 0; g < s->n_node; ++g) {
+            const long long d = s->node_inv.empty() ? g : s->node_inv[g];
+            for (int c = 0; c < 3; ++c) dst[g * 3 + c] = tmp[d * s->F + field * 3 + c];
+        }
     };
     if (u) {
         if ((st = d2h(s, tmp.data(), s->u, nF * 8))) return st;
@@ -1100,13 +1460,17 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
         if (is_real_float) {
             std::vector<float> f(nF);
             if ((st = d2h(s, f.data(), dev, nF * 4))) return st;
-            for (long long g = 0; g < s->n_node; ++g)
-                for (int c = 0; c < 3; ++c) f[g * s->F + field * 3 + c] = src ? (float)src[g * 3 + c] : 0.0f;
+            for (long long g = 0; g < s->n_node; ++g) {
+                const long long d = s->node_inv.empty() ? g : s->node_inv[g];
+                for (int c = 0; c < 3; ++c) f[d * s->F + field * 3 + c] = src ? (float)src[g * 3 + c] : 0.0f;
+            }
             if ((st = h2d(s, dev, f.data(), nF * 4))) return st;
         } else {
             if ((st = d2h(s, tmp.data(), dev, nF * 8))) return st;
-            for (long long g = 0; g < s->n_node; ++g)
-                for (int c = 0; c < 3; ++c) tmp[g * s->F + field * 3 + c] = src ? src[g * 3 + c] : 0.0;
+            for (long long g = 0; g < s->n_node; ++g) {
+                const long long d = s->node_inv.empty() ? g : s->node_inv[g];
+                for (int c = 0; c < 3; ++c) tmp[d * s->F + field * 3 + c] = src ? src[g * 3 + c] : 0.0;
+            }
             if ((st = h2d(s, dev, tmp.data(), nF * 8))) return st;
         }
         return GFB_OK;
@@ -1125,6 +1489,10 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
         CU(cudaMemset(s->npml_prev, 0, (size_t)s->n_pml_node * s->F * sizeof(float)));
     }
     if ((st = launch_predict(s))) return st;
+    {
+        std::vector<int> ms(s->n_model, step);
+        if ((st = h2d(s, s->d_mstep, ms.data(), ms.size() * 4))) return st;
+    }
     CU(cudaStreamSynchronize(s->stream));
     s->step = step;
     return GFB_OK;
@@ -1246,7 +1614,7 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
             for (int c = 0; c < 3; ++c) h[q * 4 + c] = (float)u[q * 3 + c];
         if ((st = h2d(s, s->ut, h.data(), nP * 4))) return st;
     }
-    if ((st = launch_elem(s, 0, 0.0))) return st;
+    if ((st = launch_elem(s, 0))) return st;
     CU(cudaStreamSynchronize(s->stream));
     if (precision == GFB_FP64) {
         std::vector<double> h(nP);

@@ -27,6 +27,8 @@ FLAG_CELL_PML = 1
 FLAG_RECORD_F32 = 2
 FLAG_FUSED_NODE = 4
 FLAG_POINT_KERNEL = 8
+FLAG_NO_GRAPH = 16
+FLAG_AUTOTUNE = 32
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -88,7 +90,9 @@ class Info(C.Structure):
         ("upload_bytes", C.c_int64),
         ("kernel_launches", C.c_int64),
         ("n_pml_node", C.c_int32),
-        ("reserved", C.c_int32),
+        ("elem_blocks", C.c_int32),
+        ("elem_kernel", C.c_int32),
+        ("cells_per_group", C.c_int32),
     ]
 
 
@@ -99,6 +103,19 @@ class Source(C.Structure):
         ("weights", _dp),
         ("n_stf", C.c_int32),
         ("stf", _dp),
+    ]
+
+
+class Model(C.Structure):
+    _fields_ = [
+        ("cell_begin", C.c_int32),
+        ("cell_end", C.c_int32),
+        ("node_begin", C.c_int32),
+        ("node_end", C.c_int32),
+        ("dt", C.c_double),
+        ("n_steps", C.c_int32),
+        ("n_stf", C.c_int32),
+        ("stf", C.POINTER(C.c_double)),
     ]
 
 
@@ -120,6 +137,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.gfb_advance.argtypes = [C.c_void_p, C.c_int32]
     lib.gfb_synchronize.argtypes = [C.c_void_p]
     lib.gfb_advance_profiled.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
+    lib.gfb_advance_timed.argtypes = [C.c_void_p, C.c_int32, _dp]
+    lib.gfb_create_batch.argtypes = [C.POINTER(Mesh), C.POINTER(Config), C.POINTER(Source), C.c_int32,
+                                     C.POINTER(Model), C.POINTER(C.c_void_p)]
     lib.gfb_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
     lib.gfb_current_step.argtypes = [C.c_void_p, _ip]
     lib.gfb_get_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
@@ -132,7 +152,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     for name in (
         "gfb_create", "gfb_destroy", "gfb_advance", "gfb_synchronize", "gfb_current_step",
         "gfb_get_state", "gfb_set_state", "gfb_records_pending", "gfb_read_record",
-        "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info",
+        "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
+        "gfb_create_batch",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -174,7 +195,8 @@ class Solver:
     """
 
     def __init__(self, prob: dict, dirs: Sequence[int] = (0,), precision: int = FP64,
-                 device: int = 0, record_slots: int = 4, record: bool = True, flags: int = 0):
+                 device: int = 0, record_slots: int = 4, record: bool = True, flags: int = 0,
+                 models: Optional[Sequence[dict]] = None):
         self.lib = load_library()
         keep = {}
 
@@ -229,7 +251,20 @@ class Solver:
         s.n_stf = 0 if stf is None else int(stf.size)
         s.stf = _ptr(stf, C.c_double)
         h = C.c_void_p()
-        _check(self.lib.gfb_create(C.byref(m), C.byref(c), C.byref(s), C.byref(h)))
+        if models is None:
+            _check(self.lib.gfb_create(C.byref(m), C.byref(c), C.byref(s), C.byref(h)))
+        else:
+            md = (Model * len(models))()
+            for k, d in enumerate(models):
+                st = np.ascontiguousarray(d["stf"], dtype=np.float64).ravel()
+                keep[f"stf{k}"] = st
+                md[k].cell_begin, md[k].cell_end = int(d["cell_begin"]), int(d["cell_end"])
+                md[k].node_begin, md[k].node_end = int(d["node_begin"]), int(d["node_end"])
+                md[k].dt = float(d["dt"])
+                md[k].n_steps = int(d["n_steps"])
+                md[k].n_stf = int(st.size)
+                md[k].stf = _ptr(st, C.c_double)
+            _check(self.lib.gfb_create_batch(C.byref(m), C.byref(c), C.byref(s), len(models), md, C.byref(h)))
         self.h = h
         self.n_node = m.n_node
         self.n_field = len(dirs)
@@ -239,6 +274,12 @@ class Solver:
 
     def advance(self, n_steps: int):
         _check(self.lib.gfb_advance(self.h, int(n_steps)))
+
+    def advance_timed(self, n_steps: int) -> float:
+        """Advance and return the device milliseconds of the n_steps steps."""
+        t = C.c_double(0.0)
+        _check(self.lib.gfb_advance_timed(self.h, int(n_steps), C.byref(t)))
+        return t.value
 
     def advance_profiled(self, n_steps: int):
         """Advance and return device milliseconds per phase (element, node, record)."""
@@ -307,3 +348,120 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# several independent models in one solver (gfb_create_batch)
+# ---------------------------------------------------------------------------
+
+def merge_problems(probs: Sequence[dict], n_steps: Optional[Sequence[int]] = None):
+    """One batch mesh from independent models, and the model table.
+
+    Cells, nodes, recording cells and source cells of model k follow those of
+    models 0..k-1; node ids are offset so no two models share a node.  Every
+    model keeps its own dt and source time function.  Returns (merged problem
+    dict, list of model dicts for Solver(models=...), layout dict with the
+    cell/node/recording-cell ranges of each model).
+    """
+    if not probs:
+        raise ValueError("no models")
+    ngll = int(probs[0]["ngll"])
+    strides = {int(p.get("snapshot_stride", 0)) for p in probs}
+    if any(int(p["ngll"]) != ngll for p in probs) or len(strides) != 1:
+        raise ValueError("models must share ngll and snapshot_stride")
+    cpml = [p.get("pml_coef_abar") is not None for p in probs]
+    if any(cpml) and not all(cpml):
+        raise ValueError("either every model has C-PML or none")
+    nn = ngll ** 3
+    cell_off = np.cumsum([0] + [int(p["n_cell"]) for p in probs])
+    node_off = np.cumsum([0] + [int(p["n_node"]) for p in probs])
+    rec_n = [0 if p.get("recording") is None else int(np.asarray(p["recording"]["rec_cell_local"]).size)
+             for p in probs]
+    rec_off = np.cumsum([0] + rec_n)
+
+    def cat(name, dtype):
+        if probs[0].get(name) is None:
+            return None
+        return np.concatenate([np.asarray(p[name], dtype=dtype).ravel() for p in probs])
+
+    merged = {"n_cell": int(cell_off[-1]), "n_node": int(node_off[-1]), "ngll": ngll,
+              "dt": float(probs[0]["dt"]), "snapshot_stride": strides.pop()}
+    merged["ibool"] = np.concatenate([np.asarray(p["ibool"], dtype=np.int64).ravel() + node_off[k]
+                                      for k, p in enumerate(probs)]).astype(np.int32)
+    merged["cell_ids"] = np.arange(merged["n_cell"], dtype=np.int64)
+    for name in ("dxi_dx", "jacobian", "lambda", "mu", "density", "mass", "pml_coef_alpha", "pml_coef_abar"):
+        merged[name] = cat(name, np.float64)
+    if all(p.get("damping") is not None for p in probs):
+        merged["damping"] = cat("damping", np.float64)
+    if all(cpml):
+        merged["pml_region"] = cat("pml_region", np.int32)
+    if sum(rec_n) > 0:
+        merged["recording"] = {"rec_cell_local": np.concatenate(
+            [np.asarray(p["recording"]["rec_cell_local"], dtype=np.int64) + cell_off[k]
+             for k, p in enumerate(probs) if p.get("recording") is not None]).astype(np.int32)}
+    ids, wts = [], []
+    for k, p in enumerate(probs):
+        if p.get("src_cell_ids") is None:
+            continue
+        cid = np.asarray(p.get("cell_ids", np.arange(int(p["n_cell"]))), dtype=np.int64)
+        pos = {int(c): i for i, c in enumerate(cid)}
+        for c, w in zip(np.asarray(p["src_cell_ids"], dtype=np.int64),
+                        np.asarray(p["src_weights"], dtype=np.float64).reshape(-1, nn)):
+            if int(c) in pos:  # a source cell outside the mesh is skipped, as in one model
+                ids.append(cell_off[k] + pos[int(c)])
+                wts.append(w)
+    if ids:
+        merged["src_cell_ids"] = np.asarray(ids, dtype=np.int64)
+        merged["src_weights"] = np.concatenate(wts)
+    models = []
+    for k, p in enumerate(probs):
+        ns = int(n_steps[k]) if n_steps is not None else int(p.get("nsteps", 2**31 - 1))
+        models.append({"cell_begin": int(cell_off[k]), "cell_end": int(cell_off[k + 1]),
+                       "node_begin": int(node_off[k]), "node_end": int(node_off[k + 1]),
+                       "dt": float(p["dt"]), "n_steps": ns,
+                       "stf": np.asarray(p.get("stf", np.zeros(0)), dtype=np.float64)})
+    layout = {"cell_off": cell_off, "node_off": node_off, "rec_off": rec_off}
+    return merged, models, layout
+
+
+class BatchSolver(Solver):
+    """Several independent models advanced together by one solver.
+
+    ``probs`` are per-model problem dicts (gfb.mesh.build_problem layout);
+    ``n_steps`` the steps each model takes (default: its "nsteps").  The
+    models share ngll, snapshot stride, precision and wavefield directions.
+    """
+
+    def __init__(self, probs: Sequence[dict], dirs: Sequence[int] = (0,), precision: int = FP64,
+                 device: int = 0, record_slots: int = 4, flags: int = 0, n_steps: Optional[Sequence[int]] = None):
+        merged, models, layout = merge_problems(probs, n_steps)
+        super().__init__(merged, dirs=dirs, precision=precision, device=device, record_slots=record_slots,
+                         flags=flags, models=models)
+        self.models = models
+        self.layout = layout
+        self.n_model = len(models)
+
+    def model_state(self, k: int, field: int = 0):
+        u, v, a = self.state(field)
+        a0, a1 = self.layout["node_off"][k], self.layout["node_off"][k + 1]
+        return u[a0:a1], v[a0:a1], a[a0:a1]
+
+    def drain_models(self):
+        """Pending snapshots split by model: list over models of
+        {field: {"steps", "strain", "u", "v", "a"}}, keeping the snapshots of
+        steps each model has taken."""
+        snaps = self.drain()
+        out = []
+        for k in range(self.n_model):
+            r0, r1 = self.layout["rec_off"][k], self.layout["rec_off"][k + 1]
+            per = {}
+            for f, d in snaps.items():
+                steps = np.asarray(d["steps"])
+                keep = steps < self.models[k]["n_steps"]
+                per[f] = {"steps": steps[keep]}
+                for name in ("strain", "u", "v", "a"):
+                    x = np.asarray(d[name])
+                    per[f][name] = x[keep][:, r0:r1] if x.size else x
+            out.append(per)
+        return out
+

@@ -235,17 +235,31 @@ def gll_geometry(corners: np.ndarray, order: int, chunk: int = 65536):
     coords = np.empty((n_cell, nn, 3))
     jac = np.empty((n_cell, nn))
     dxi = np.empty((n_cell, nn, 9))
+    # shape-function products as matrix products over all cells of a chunk
+    dSm = np.ascontiguousarray(dS.transpose(0, 2, 1).reshape(nn * 3, 8))  # [(n, m), a]
     for c0 in range(0, n_cell, chunk):
         cv = corners[c0 : c0 + chunk]
-        coords[c0 : c0 + chunk] = np.einsum("na,eac->enc", S, cv)
+        ne = cv.shape[0]
+        xa = np.ascontiguousarray(cv.transpose(1, 0, 2).reshape(8, ne * 3))  # [a, (e, c)]
+        coords[c0 : c0 + chunk] = (S @ xa).reshape(nn, ne, 3).transpose(1, 0, 2)
         # J[m, c] = sum_a dS[a, m] x_a[c]  (J = dS.T @ corners, gll_geometry.py:173)
-        J = np.einsum("nam,eac->enmc", dS, cv)
-        det = np.linalg.det(J)
+        J = (dSm @ xa).reshape(nn, 3, ne, 3).transpose(2, 0, 1, 3)  # [e, n, m, c]
+        a, b, c = J[..., 0, 0], J[..., 0, 1], J[..., 0, 2]
+        d, e, f = J[..., 1, 0], J[..., 1, 1], J[..., 1, 2]
+        g, h, i = J[..., 2, 0], J[..., 2, 1], J[..., 2, 2]
+        # determinant and inverse by cofactors (equal to LU-based det/inv to
+        # rounding; the reference's np.linalg calls differ from these only in
+        # the last bits)
+        A, B, C = e * i - f * h, f * g - d * i, d * h - e * g
+        det = a * A + b * B + c * C
         jac[c0 : c0 + chunk] = det
-        inv = np.zeros_like(J)
         ok = det > 0
-        inv[ok] = np.linalg.inv(J[ok])
-        dxi[c0 : c0 + chunk] = inv.reshape(-1, nn, 9)
+        rdet = np.where(ok, 1.0 / np.where(ok, det, 1.0), 0.0)
+        inv = np.empty((ne, nn, 9))
+        inv[..., 0], inv[..., 1], inv[..., 2] = A * rdet, (c * h - b * i) * rdet, (b * f - c * e) * rdet
+        inv[..., 3], inv[..., 4], inv[..., 5] = B * rdet, (a * i - c * g) * rdet, (c * d - a * f) * rdet
+        inv[..., 6], inv[..., 7], inv[..., 8] = C * rdet, (b * g - a * h) * rdet, (a * e - b * d) * rdet
+        dxi[c0 : c0 + chunk] = inv
     wijk = (w[:, None, None] * w[None, :, None] * w[None, None, :]).ravel()
     mass = jac * wijk[None, :]
     return (
@@ -495,12 +509,22 @@ def cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt):
     regions = cpml_regions(coords, is_pml, bounds, widths)
     K, d, al = cpml_profiles(coords, is_pml, regions, bounds, widths, vp, f0)
     n_cell, nn = K.shape[0], K.shape[1]
-    coef_alpha = np.zeros((n_cell, nn, 9))
+    # outside C-PML cells alpha = 0, whose coefficients are (1, dt/2, dt/2)
+    # exactly (the |b| < MIN_DISTANCE series at b = 0)
+    c0z, c1z, c2z = convolution_coef(np.zeros(1), dt)
+    coef_alpha = np.empty((n_cell, nn, 9))
     for axis in range(3):
-        c0, c1, c2 = convolution_coef(al[:, :, axis], dt)
-        coef_alpha[:, :, axis * 3 + 0] = c0.reshape(n_cell, nn)
-        coef_alpha[:, :, axis * 3 + 1] = c1.reshape(n_cell, nn)
-        coef_alpha[:, :, axis * 3 + 2] = c2.reshape(n_cell, nn)
+        coef_alpha[:, :, axis * 3 + 0] = c0z[0]
+        coef_alpha[:, :, axis * 3 + 1] = c1z[0]
+        coef_alpha[:, :, axis * 3 + 2] = c2z[0]
+    idx = np.nonzero(is_pml)[0]
+    for axis in range(3):
+        if idx.size == 0:
+            break
+        c0, c1, c2 = convolution_coef(al[idx, :, axis], dt)
+        coef_alpha[idx, :, axis * 3 + 0] = c0.reshape(idx.size, nn)
+        coef_alpha[idx, :, axis * 3 + 1] = c1.reshape(idx.size, nn)
+        coef_alpha[idx, :, axis * 3 + 2] = c2.reshape(idx.size, nn)
     abar = abar_coefficients(K, d, al, regions)
     return regions, coef_alpha, abar
 

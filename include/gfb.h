@@ -102,6 +102,15 @@ typedef struct gfb_config {
  * the thread-per-xi-line kernel (same arithmetic, different summation order;
  * for comparisons). */
 #define GFB_FLAG_POINT_KERNEL 8
+/* Launch each step's kernels one by one instead of replaying the step as a
+ * captured CUDA graph. */
+#define GFB_FLAG_NO_GRAPH 16
+/* At the end of gfb_create(_batch), time full colour sweeps of each FP32
+ * element-kernel candidate (the line kernel with each cells-per-group count
+ * it is built with, and the thread-per-point kernel) on this mesh and keep
+ * the fastest; gfb_get_info reports the choice.  Tuning leaves the state
+ * unchanged. */
+#define GFB_FLAG_AUTOTUNE 32
 
 /* Point-force source (config.h5 /source, io.cpp:681-707). */
 typedef struct gfb_source {
@@ -131,6 +140,36 @@ const char* gfb_last_error(void);
 gfb_status gfb_create(const gfb_mesh* mesh, const gfb_config* config, const gfb_source* source,
                       gfb_solver** out);
 
+/*
+ * One of several independent models held by one solver (no counterpart in
+ * the reference, which runs one model per process).  The batch mesh passed to
+ * gfb_create_batch is the models' meshes one after the other: model k owns
+ * cells [cell_begin, cell_end) and nodes [node_begin, node_end), and its
+ * cells use only its nodes.  Source cells are found by cell_ids over the
+ * whole batch mesh; each model has its own time step and source time
+ * function.  A model takes n_steps steps; after that gfb_advance leaves its
+ * state as it is while the other models go on.
+ */
+typedef struct gfb_model {
+    int32_t cell_begin, cell_end;
+    int32_t node_begin, node_end;
+    double dt;
+    int32_t n_steps;
+    int32_t n_stf;
+    const double* stf;         /* [n_stf] this model's stf_values              */
+} gfb_model;
+
+/*
+ * gfb_create for n_model (1..255) models advanced together: one element
+ * launch per colour covers the cells of every model, so many small models
+ * fill the GPU as one large one does.  config->dt is not used (each model's
+ * dt is); the snapshot stride, precision and wavefield directions are shared.
+ * gfb_get_state / gfb_read_record return the batch's node and recording-cell
+ * arrays, model after model.
+ */
+gfb_status gfb_create_batch(const gfb_mesh* mesh, const gfb_config* config, const gfb_source* source,
+                            int32_t n_model, const gfb_model* models, gfb_solver** out);
+
 /* Release all device and host memory.  Replaces cuda_free_state
  * (cuda_step.hpp:80-81). */
 gfb_status gfb_destroy(gfb_solver* solver);
@@ -150,6 +189,12 @@ gfb_status gfb_destroy(gfb_solver* solver);
  * oldest is moved to ordinary host memory, so none is lost.
  */
 gfb_status gfb_advance(gfb_solver* solver, int32_t n_steps);
+
+/*
+ * gfb_advance with one pair of CUDA events on the solver's stream around the
+ * n_steps steps; adds their device milliseconds to *ms and synchronises.
+ */
+gfb_status gfb_advance_timed(gfb_solver* solver, int32_t n_steps, double* ms);
 
 /*
  * gfb_advance with CUDA events on the solver's stream around each phase of
@@ -175,7 +220,9 @@ typedef struct gfb_info {
     int64_t upload_bytes;    /* bytes copied host->device by gfb_create                    */
     int64_t kernel_launches; /* kernels launched by this solver so far                     */
     int32_t n_pml_node;      /* global nodes carrying C-PML state (0: per-cell form)        */
-    int32_t reserved;
+    int32_t elem_blocks;     /* blocks in the persistent grid of the element kernel in use  */
+    int32_t elem_kernel;     /* 1: thread-per-xi-line kernel, 0: thread-per-point kernel    */
+    int32_t cells_per_group; /* cells per block iteration of the line kernel (0 otherwise)  */
 } gfb_info;
 
 gfb_status gfb_get_info(const gfb_solver* solver, gfb_info* info);
