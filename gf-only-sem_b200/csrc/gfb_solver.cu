@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/gfb.h"
+#include "gfb_internal.h"
 #include "gfb_kernels.cuh"
 
 namespace {
@@ -118,9 +119,10 @@ struct DevBuf {
 struct Snapshot {
     int step;
     int slot;                  // ring slot (device + pinned host), -1 once spilled
-    std::vector<double> host;  // spilled copy [NFLD][n_rec][NN][15]
+    std::vector<unsigned char> host;  // spilled raw copy [NFLD][n_rec][NN][15] (float or double)
     int fields_read = 0;
     int readers = 0;           // gfb_read_record calls copying out of the slot
+    bool done = false;         // read (or released); removed once no reader holds it
     std::vector<char> read_mask;
 };
 
@@ -178,6 +180,7 @@ struct gfb_solver {
     void *d_mstf = nullptr, *d_stf_all = nullptr;
     bool use_graph = true;
     cudaGraphExec_t gexec = nullptr;   // one step: step start, colours, node pass
+    gfb::Layer* layer = nullptr;       // learned absorbing layer (or none)
     long long graph_launches = 0;
     void* ring = nullptr;              // device snapshot ring [slots]
     std::vector<void*> pinned;         // pinned host copy of each slot
@@ -213,6 +216,7 @@ struct gfb_solver {
     }
     ~gfb_solver() {
         if (gexec) cudaGraphExecDestroy(gexec);
+        if (layer) gfb::layer_free(layer);
         for (auto e : rec_evt) cudaEventDestroy(e);
         for (auto e : copy_evt) cudaEventDestroy(e);
         for (auto p : pinned) cudaFreeHost(p);
@@ -619,22 +623,24 @@ gfb_status launch_predict(gfb_solver* s) {
 size_t snapshot_values(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
 size_t snapshot_bytes(const gfb_solver* s) { return snapshot_values(s) * (s->rec_f32 ? 4 : 8); }
 
-// Convert n snapshot values starting at value `off` of a pinned slot to double.
-void slot_values(const gfb_solver* s, int slot, size_t off, size_t n, double* dst) {
+// Convert n snapshot values starting at value `off` of a raw snapshot
+// (float or double, as recorded) to double.
+void raw_values(const gfb_solver* s, const void* raw, size_t off, size_t n, double* dst) {
     if (s->rec_f32) {
-        const float* src = static_cast<const float*>(s->pinned[slot]) + off;
+        const float* src = static_cast<const float*>(raw) + off;
         for (size_t i = 0; i < n; ++i) dst[i] = src[i];
     } else {
-        std::memcpy(dst, static_cast<const double*>(s->pinned[slot]) + off, n * sizeof(double));
+        std::memcpy(dst, static_cast<const double*>(raw) + off, n * sizeof(double));
     }
 }
 
-// Copy a snapshot out of its pinned slot into pageable memory so the slot can
-// take a new snapshot (only when the caller has not read it yet).
+// Copy a snapshot out of its pinned slot into pageable memory, as recorded,
+// so the slot can take a new snapshot (only when the caller has not read it
+// yet).
 gfb_status spill(gfb_solver* s, Snapshot& snap) {
     CU(cudaEventSynchronize(s->copy_evt[snap.slot]));
-    snap.host.resize(snapshot_values(s));
-    slot_values(s, snap.slot, 0, snap.host.size(), snap.host.data());
+    snap.host.resize(snapshot_bytes(s));
+    std::memcpy(snap.host.data(), s->pinned[snap.slot], snap.host.size());
     snap.slot = -1;
     return GFB_OK;
 }
@@ -1035,6 +1041,7 @@ gfb_status step_body(gfb_solver* s, cudaEvent_t* ev) {
     if (st) return st;
     for (int c = 0; c < n_colour; ++c)
         if ((st = launch_elem(s, c))) return st;
+    if (s->layer && (st = gfb::layer_step(s, s->layer))) return st;
     if (ev) CU(cudaEventRecord(ev[1], s->stream));
     if (!s->fuse)
         if ((st = launch_node(s))) return st;
@@ -1081,15 +1088,34 @@ gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
         // memory first.  The record kernel waits (on the GPU) for the last
         // device->host copy out of the slot; the copy of this snapshot runs
         // on the copy stream, overlapped with the following steps.
-        std::unique_lock<std::mutex> lk(s->rec_mu);
+        // keep the host at most half the ring ahead of the snapshot copies, so
+        // a reader thread gets the time to release a slot before it is
+        // needed again (replayed steps are queued much faster than they run)
         const int slot = s->next_slot;
+        if (s->slots > 1) {
+            const int back = (slot - s->slots / 2 + s->slots) % s->slots;
+            if (s->copy_issued[back]) CU(cudaEventSynchronize(s->copy_evt[back]));
+        }
+        std::unique_lock<std::mutex> lk(s->rec_mu);
         s->next_slot = (s->next_slot + 1) % s->slots;
-        for (auto& old : s->pending)
-            if (old.slot == slot) {
-                s->rec_cv.wait(lk, [&] { return old.readers == 0; });  // a reader is copying it out
-                if (old.slot == slot)
-                    if ((st = spill(s, old))) return st;
+        for (;;) {
+            // the unread snapshot still in this slot, looked up again after
+            // every wait (a reader may have released and removed it)
+            while (!s->pending.empty() && s->pending.front().done && s->pending.front().readers == 0)
+                s->pending.pop_front();
+            Snapshot* old = nullptr;
+            for (auto& p : s->pending)
+                if (p.slot == slot) {
+                    old = &p;
+                    break;
+                }
+            if (!old) break;
+            if (old->readers > 0) {
+                s->rec_cv.wait(lk);  // a reader is copying it out
+                continue;
             }
+            if ((st = spill(s, *old))) return st;
+        }
         if (s->copy_issued[slot]) CU(cudaStreamWaitEvent(s->stream, s->copy_evt[slot], 0));
         void* dslot = static_cast<unsigned char*>(s->ring) + (size_t)slot * snapshot_bytes(s);
         if ((st = launch_record(s, dslot))) return st;
@@ -1501,7 +1527,9 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
 gfb_status gfb_records_pending(gfb_solver* s, int32_t* n) {
     if (!s || !n) return fail(GFB_ERR_INVALID, "NULL argument");
     std::lock_guard<std::mutex> lk(s->rec_mu);
-    *n = (int32_t)s->pending.size();
+    int32_t k = 0;
+    for (const auto& p : s->pending) k += p.done ? 0 : 1;
+    *n = k;
     return GFB_OK;
 }
 
@@ -1515,8 +1543,10 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
     int slot;
     {
         std::lock_guard<std::mutex> lk(s->rec_mu);
-        if (s->pending.empty()) return fail(GFB_ERR_STATE, "no snapshot pending");
-        snap = &s->pending.front();
+        auto it = s->pending.begin();
+        while (it != s->pending.end() && it->done) ++it;  // read, still held by another reader
+        if (it == s->pending.end()) return fail(GFB_ERR_STATE, "no snapshot pending");
+        snap = &*it;
         snap->readers++;  // keeps the slot from being spilled or reused while copying
         slot = snap->slot;
     }
@@ -1525,15 +1555,13 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
     const double* src = nullptr;
     const bool want = strain || u || v || a;
     gfb_status st = GFB_OK;
-    if (slot >= 0) {
-        if (cudaEventSynchronize(s->copy_evt[slot]) != cudaSuccess) st = fail(GFB_ERR_CUDA, "snapshot copy failed");
-        if (want) {
-            buf.resize(per_field);
-            if (!st) slot_values(s, slot, field * per_field, per_field, buf.data());
-            src = buf.data();
-        }
-    } else {
-        src = snap->host.data() + field * per_field;
+    if (slot >= 0 && cudaEventSynchronize(s->copy_evt[slot]) != cudaSuccess)
+        st = fail(GFB_ERR_CUDA, "snapshot copy failed");
+    if (want) {
+        buf.resize(per_field);
+        if (!st) raw_values(s, slot >= 0 ? s->pinned[slot] : (const void*)snap->host.data(), field * per_field,
+                            per_field, buf.data());
+        src = buf.data();
     }
     if (step) *step = snap->step;
     if (!st && want) {
@@ -1557,8 +1585,10 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
                 snap->read_mask[field] = 1;
                 snap->fields_read++;
             }
-            if (release || snap->fields_read == s->nfld) s->pending.pop_front();
+            if (release || snap->fields_read == s->nfld) snap->done = true;
         }
+        while (!s->pending.empty() && s->pending.front().done && s->pending.front().readers == 0)
+            s->pending.pop_front();
     }
     s->rec_cv.notify_all();
     return st;
@@ -1651,6 +1681,42 @@ gfb_status set_error(gfb_status st, const char* msg) { return fail(st, "%s", msg
 bool gll_tables_for(int ngll, std::vector<double>& w, std::vector<double>& D) {
     std::vector<double> x;
     return gll_tables(ngll - 1, x, w, D);
+}
+
+SolverView solver_view(gfb_solver* s) {
+    SolverView v;
+    v.device = s->device;
+    v.stream = s->stream;
+    v.precision = s->prec;
+    v.n_field = s->nfld;
+    v.n_model = s->n_model;
+    v.n_node = s->n_node;
+    v.dt = s->dt;
+    v.u = s->u;
+    v.v = s->v;
+    v.a = s->a;
+    v.ut = s->ut;
+    v.force = s->force;
+    v.mass = s->mass;
+    v.mstep = s->d_mstep;
+    v.node_inv = &s->node_inv;
+    v.node_perm = &s->node_perm;
+    return v;
+}
+
+gfb_status solver_predict(gfb_solver* s) { return launch_predict(s); }
+
+Layer* solver_layer(gfb_solver* s) { return s->layer; }
+
+gfb_status solver_set_layer(gfb_solver* s, Layer* layer) {
+    if (s->layer) layer_free(s->layer);
+    s->layer = layer;
+    // the captured step graph does not contain the layer's launch
+    if (s->gexec) {
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
+    return GFB_OK;
 }
 
 }  // namespace gfb

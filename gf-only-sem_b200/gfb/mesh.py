@@ -584,8 +584,13 @@ def locate_point_source(coords, corners, source_xyz, is_pml, order):
     return np.array(ids, dtype=np.int64), np.array([w / total for w in ws]).reshape(len(ids), ng, ng, ng)
 
 
-def recording_map(coords, ibool, is_pml, bounds, record_depth_max_m):
-    """Recording cells and GLL node map (recording_map.py:18-170), single rank."""
+def recording_map(coords, ibool, is_pml, bounds, record_depth_max_m, tile=None, nxy=None):
+    """Recording cells and GLL node map (recording_map.py:18-170), single rank.
+
+    ``tile`` = (i0, j0, n) records instead the top cell of each column
+    i0..i0+n-1, j0..j0+n-1 (``nxy`` = (nx, ny) cells per row): a tile of n x n
+    surface elements for strain Green's function extraction, which follows
+    the free surface where it is not flat."""
     n_cell, ng = coords.shape[0], coords.shape[1]
     nn = ng**3
     zmin, zmax = bounds["zmin"], bounds["zmax"]
@@ -597,6 +602,12 @@ def recording_map(coords, ibool, is_pml, bounds, record_depth_max_m):
     actual = float(above[0] - zmin) if above.size else float(zmax - zmin)
     cen = coords.reshape(n_cell, nn, 3).mean(axis=1)
     sel = (~is_pml) & (cen[:, 2] <= zmin + actual + 1e-12)
+    if tile is not None:
+        i0, j0, n = tile
+        e = np.arange(n_cell)
+        ci, cj, ck = e % nxy[0], (e // nxy[0]) % nxy[1], e // (nxy[0] * nxy[1])
+        sel = (~is_pml) & (ck == 0) & (ci >= i0) & (ci < i0 + n) & (cj >= j0) & (cj < j0 + n)
+        actual = float((cz.max(axis=1) - cz.min(axis=1))[sel].max()) if sel.any() else 0.0
     rec_cell = np.nonzero(sel)[0].astype(np.int32)
     nodes = ibool.reshape(n_cell, nn)[rec_cell]
     gll_ids, first, inv = np.unique(nodes.ravel(), return_index=True, return_inverse=True)
@@ -654,6 +665,44 @@ def layered(depths, vps, vss, rhos) -> MaterialFn:
     return f
 
 
+def gaussian_field(lo, hi, corr_len: float, seed: int, spacing: Optional[float] = None):
+    """Seeded random field with Gaussian correlation exp(-r^2/corr_len^2),
+    unit variance, clipped to +-1, on a regular grid over the box [lo, hi];
+    returns f(coords) -> values by trilinear interpolation.
+
+    White noise filtered by a Gaussian kernel of standard deviation
+    corr_len/2 has exactly that correlation function."""
+    from scipy import ndimage
+
+    lo, hi = np.asarray(lo, dtype=np.float64), np.asarray(hi, dtype=np.float64)
+    h = spacing if spacing is not None else corr_len / 3.0
+    shape = tuple(int(np.ceil((hi[a] - lo[a]) / h)) + 2 for a in range(3))
+    rng = np.random.default_rng(seed)
+    g = ndimage.gaussian_filter(rng.standard_normal(shape), sigma=0.5 * corr_len / h, mode="wrap")
+    g = np.clip(g / g.std(), -1.0, 1.0)
+
+    def f(c):
+        flat = np.asarray(c, dtype=np.float64).reshape(-1, 3)
+        out = np.empty(flat.shape[0])
+        for a0 in range(0, flat.shape[0], 1 << 22):
+            x = ((flat[a0 : a0 + (1 << 22)] - lo) / h).T
+            out[a0 : a0 + (1 << 22)] = ndimage.map_coordinates(g, x, order=1, mode="nearest")
+        return out.reshape(np.shape(c)[:-1])
+
+    return f
+
+
+def perturbed(base: "MaterialFn", field, amp: float = 0.1) -> "MaterialFn":
+    """Background model with its velocities scaled by (1 + amp * field)."""
+
+    def f(c):
+        vp, vs, rho = base(c)
+        s = 1.0 + amp * field(c)
+        return vp * s, vs * s, rho
+
+    return f
+
+
 def seeded_layers(seed: int, lz: float, n_layers: int = 3):
     """Three flat layers with seeded interfaces and (vp, vp/vs, rho) in
     vp 3000-7000 m/s, vp/vs 1.6-1.9, rho 2200-3000 kg/m^3; vp grows with depth."""
@@ -679,6 +728,7 @@ def build_problem(
     t0: float = 1.0,
     amp: float = 1.0e20,
     with_cpml: bool = True,
+    record_tile=None,
 ) -> dict:
     """Every solver input for one synthetic model, reference layouts."""
     V = vertex_grid(spec)
@@ -745,5 +795,6 @@ def build_problem(
     out["stf_t"] = t
     out["stf"] = ricker(t, f0=f0, t0=t0, amp=amp)
     if record_depth_max_m > 0.0:
-        out["recording"] = recording_map(coords, ibool, is_pml, bounds, record_depth_max_m)
+        out["recording"] = recording_map(coords, ibool, is_pml, bounds, record_depth_max_m, tile=record_tile,
+                                         nxy=(spec.nx, spec.ny))
     return out

@@ -311,6 +311,96 @@ gfb_status gfb_element_residual_noalloc(int32_t n_elem, const double* dxi_dx, co
                                         const double* lambda_, const double* mu, int32_t ngll,
                                         const double* u, double* r, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned absorbing layer (no counterpart in the reference, which truncates
+ * the domain with C-PML, pml.cpp, or the legacy damping layer).
+ *
+ * A thin domain (the model plus a one-element C-PML layer) gets a force
+ * correction at the nodes of its layer cells from a small network per node
+ * class ("net"): inputs are u, v, a of the node (in the node's face frame,
+ * each channel divided by its scale) over the last 4 steps, 36 values;
+ * hidden layers relu(+-W1 x) and relu(W2 h) of 64; output W3 h in the face
+ * frame; correction = s_c (f(x) - f(-x)) / 2 (bias-free, so the correction
+ * scales with the wavefield).  Weights are BF16 and inference runs on the
+ * tensor cores with FP32 accumulation, between the element and node phases
+ * of every step.  The networks are trained on the GPU from replays of a
+ * thick-C-PML run of the enlarged domain: the thick run's state is copied
+ * into the thin solver each step and the target is m (a_thick - a_thin).
+ * A monitor keeps the running mean over recent steps of (work done by the
+ * correction) / (kinetic energy of the layer nodes); above the threshold,
+ * or on a non-finite value, the correction is switched off for good and the
+ * layer is plain one-element C-PML (the fallback).
+ * ------------------------------------------------------------------------ */
+#define GFB_LAYER_NIN 36
+#define GFB_LAYER_NHID 64
+#define GFB_LAYER_NOUT 3
+/* FP32 parameters of one network: W1 [64][36], W2 [64][64], W3 [3][64] */
+#define GFB_LAYER_PARAMS 6592
+/* BF16 values of one network in the inference layout (gfb_layer_pack) */
+#define GFB_LAYER_WEIGHTS 8768
+
+typedef struct gfb_layer {
+    int32_t n_node;          /* layer nodes carrying a correction            */
+    const int32_t* node;     /* [n_node] node ids of the solver's mesh       */
+    const int8_t* frame;     /* [n_node][3]: local axis j is global axis
+                                |frame[j]|-1 taken with the sign of frame[j]
+                                (local axis 0 = outward normal)              */
+    const uint8_t* net;      /* [n_node] network of the node, < n_net        */
+    int32_t n_net;           /* 1..64                                        */
+} gfb_layer;
+
+/* BF16 inference layout [n_net][GFB_LAYER_WEIGHTS] from FP32 parameters
+ * [n_net][GFB_LAYER_PARAMS] (round to nearest even). */
+gfb_status gfb_layer_pack(int32_t n_net, const float* params, uint16_t* weights);
+
+/* Attach a trained layer to an FP32 single-model solver (replaces any
+ * previous one).  scales = {u, v, a channel scales, output scale};
+ * threshold = fallback limit of the monitored residual. */
+gfb_status gfb_layer_attach(gfb_solver* solver, const gfb_layer* layer, const uint16_t* weights,
+                            const float* scales, double threshold);
+
+/* Whether the correction is still applied, and the monitored residual. */
+gfb_status gfb_layer_status(gfb_solver* solver, int32_t* active, double* residual);
+
+typedef struct gfb_trainer gfb_trainer;
+
+/* Trainer with room for `capacity` samples per network on `device`; seeded
+ * He initialisation of the FP32 parameters. */
+gfb_status gfb_trainer_create(int32_t n_net, int64_t capacity, int32_t device, uint64_t seed,
+                              gfb_trainer** out);
+gfb_status gfb_trainer_destroy(gfb_trainer* trainer);
+
+/* Replay n_steps steps: before each step the thin solver's state is set to
+ * the thick solver's on the shared nodes (thin_to_thick maps thin node ids
+ * to thick node ids), both solvers step, and every sample_stride-th step
+ * the (features, target) pairs of every node_stride-th layer node are added
+ * to the data set.  Both solvers: FP32, same wavefields, same step, no layer
+ * attached to the thin one. */
+gfb_status gfb_trainer_collect(gfb_trainer* trainer, gfb_solver* thin, gfb_solver* thick,
+                               const int32_t* thin_to_thick, const gfb_layer* layer, int32_t n_steps,
+                               int32_t sample_stride, int32_t node_stride);
+
+/* Samples held per network [n_net]. */
+gfb_status gfb_trainer_samples(gfb_trainer* trainer, int64_t* counts);
+
+/* Channel scales (set before fitting; otherwise the RMS of the collected
+ * u, v, a features and targets). */
+gfb_status gfb_trainer_set_scales(gfb_trainer* trainer, const float* scales);
+
+/* Adam on the mean squared error of per-sample normalised (features,
+ * targets); loss[epochs] receives the mean loss of each epoch. */
+gfb_status gfb_trainer_fit(gfb_trainer* trainer, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                           double* loss);
+
+/* Gradient of the summed loss over n given samples (raw face-frame features
+ * [n][36], targets [n][3]) for network `net` at the current parameters. */
+gfb_status gfb_trainer_gradient(gfb_trainer* trainer, int32_t net, int32_t n, const float* x, const float* y,
+                                float* grad, double* loss);
+
+/* FP32 parameters [n_net][GFB_LAYER_PARAMS] and scales [4]. */
+gfb_status gfb_trainer_get_params(gfb_trainer* trainer, float* params, float* scales);
+gfb_status gfb_trainer_set_params(gfb_trainer* trainer, const float* params);
+
 /*
  * File-level driver: run the forward solve of one direction with the
  * reference's CWD-relative file contract (solver.cpp:73-739,

@@ -137,6 +137,30 @@ def test_fp32_batched_within_1e4_of_fp64_oracle():
         compare_runs(snaps[d], ref, FP32_TOL, f"fp32 field {d}")
 
 
+def deformed_problem(nsteps):
+    """Jittered interior vertices, sinusoid topography, a Gaussian-correlated
+    velocity perturbation and a recording tile that follows the surface (the
+    construction of the 128 x 128 x 64 deformed workload at 7 x 6 x 5 cells)."""
+    spec = mesh.MeshSpec(nx=7, ny=6, nz=5, dx=200.0, dy=200.0, dz=200.0, order=4, jitter=0.1, topo_terms=8,
+                         topo_amp=150.0, seed=9, pml={"xmin": 1, "xmax": 1, "ymin": 1, "ymax": 1, "zmax": 1})
+    field = mesh.gaussian_field((-200.0, -200.0, -200.0), (1600.0, 1400.0, 1500.0), 150.0, 10)
+    mat = mesh.perturbed(mesh.seeded_layers(9, 1000.0), field, 0.1)
+    return mesh.build_problem(spec, mat, np.array([700.0, 600.0, 450.0]), nsteps=nsteps, snapshot_stride=10,
+                              record_depth_max_m=200.0, record_tile=(1, 1, 4))
+
+
+def test_fp32_deformed_perturbed_mesh_within_1e4_of_fp64_oracle():
+    prob = deformed_problem(250)
+    assert prob["recording"]["rec_cell_local"].size == 16
+    n = prob["nsteps"]
+    s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32)
+    s.advance(n)
+    snaps = s.drain()
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(snaps[d], ref, FP32_TOL, f"deformed fp32 field {d}")
+
+
 def test_fp32_node_and_cell_cpml_forms_agree():
     """The FP32 path keeps C-PML memory per global node when the cells agree
     on each axis's coefficients at shared nodes; the per-cell form
