@@ -68,6 +68,16 @@ WORKLOADS = {
 BATCH = dict(n_model=32, seed=4, d=250.0, pml=4, nmin=(16, 16, 8), nmax=(48, 48, 24), f0=(1.0, 3.0),
              steps=(1000, 3000), stride=50)
 
+# learned one-element absorbing layer on a 96 x 96 x 48 layered
+# model (interior 94 x 94 x 47), judged against the same interior with a
+# 10-element C-PML; networks trained on replays of small seeded models
+LAYER = {
+    "layer96": dict(ni=94, nk=47, d=250.0, seed=2, steps=2000, stride=10,
+                    train_pairs=24, train_ni=10, train_nk=6, train_steps=700, epochs=30),
+    "layer24": dict(ni=22, nk=11, d=250.0, seed=2, steps=900, stride=10,
+                    train_pairs=6, train_ni=8, train_nk=5, train_steps=500, epochs=15),
+}
+
 METRIC = "GLL-point updates/s (FP32 batched x/y/z, 1 B200)"
 UNIT = "GLL-pt/s"
 
@@ -186,6 +196,88 @@ def run_batch(args):
         "per_model": per_model,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_layer(args):
+    """Learned absorbing layer: train on replays, then the reflection error of
+    the thin domain with and without the learned layer against the thick
+    C-PML run, at the recorded interior surface cells."""
+    import gfb
+    from gfb import layer as gl
+
+    w = LAYER[args.workload]
+    rng = np.random.default_rng(w["seed"])
+    d = w["d"]
+
+    def pair(seed, ni, nk, steps):
+        r = np.random.default_rng(seed)
+        return gl.PairSpec(ni=ni, nj=ni, nk=nk, d=d, seed=seed, f0=float(r.uniform(1.5, 2.5)),
+                           src=(float(r.uniform(1.5, ni - 1.5) * d), float(r.uniform(1.5, ni - 1.5) * d),
+                                float(r.uniform(1.0, nk - 1.5) * d)), nsteps=steps)
+
+    t0 = time.perf_counter()
+    p0 = pair(1, w["train_ni"], w["train_nk"], 10)
+    n_net = gl.Layer(gl.build_domain(p0, 1)).n_net
+    tr = gl.Trainer(n_net=n_net, capacity=8_000_000, device=args.device, seed=1)
+    for k in range(w["train_pairs"]):
+        gl.collect_pair(tr, pair(1000 + k, w["train_ni"], w["train_nk"], w["train_steps"]), sample_stride=3,
+                        node_stride=2, device=args.device)
+    t_collect = time.perf_counter() - t0
+    base = tr.baseline_loss()
+    t0 = time.perf_counter()
+    loss = tr.fit(w["epochs"], batch=2048, lr=1e-3, seed=3)
+    t_fit = time.perf_counter() - t0
+    params, scales = tr.params()
+    samples = int(tr.samples().sum())
+    tr.close()
+
+    p = pair(w["seed"], w["ni"], w["nk"], w["steps"])
+    thin, thick, _ = gl.build_pair(p)
+    shift = (p.n_thick - p.n_thin) * d
+
+    def run(prob, learned):
+        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, device=args.device, record_slots=16,
+                       flags=gfb.FLAG_RECORD_F32)
+        if learned:
+            gl.attach(s, gl.Layer(prob), params, scales, threshold=0.05)
+        consumer_snaps = []
+        ms = 0.0
+        done = 0
+        while done < w["steps"]:
+            k = min(200, w["steps"] - done)
+            ms += s.advance_timed(k)
+            consumer_snaps.append(s.drain())
+            done += k
+        st = gl.status(s) if learned else None
+        s.close()
+        snaps = {f: {key: np.concatenate([np.asarray(c[f][key]) for c in consumer_snaps]) for key in
+                     ("steps", "strain", "u", "v", "a")} for f in range(3)}
+        return snaps, ms / w["steps"], st
+
+    judge, ms_thick, _ = run(thick, False)
+    plain, ms_plain, _ = run(thin, False)
+    learned, ms_learned, st = run(thin, True)
+    err_plain = [gl.reflection_error(thin, plain[f], thick, judge[f], shift) for f in range(3)]
+    err_learned = [gl.reflection_error(thin, learned[f], thick, judge[f], shift) for f in range(3)]
+    value = float(np.sqrt(np.mean(np.square(err_learned))))
+    line = {
+        "metric": "reflection error of a learned 1-element absorbing layer vs a 10-element C-PML "
+                  "(rel L2 of recorded surface displacement, x/y/z)",
+        "value": value, "unit": "rel L2", "n_gpus": 1, "steps": w["steps"], "warmup": 0,
+        "ms_per_step": ms_learned, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 solver, bf16 network weights", "data": "synthetic",
+        "config": {"workload": args.workload, "thin_cells": thin["n_cell"], "thick_cells": thick["n_cell"],
+                   "fewer_elements": 1.0 - thin["n_cell"] / thick["n_cell"],
+                   "train_pairs": w["train_pairs"], "train_samples": samples, "epochs": w["epochs"],
+                   "loss_zero_prediction": base, "loss_first_epoch": float(loss[0]) if len(loss) else None,
+                   "loss_last_epoch": float(loss[-1]) if len(loss) else None,
+                   "collect_s": t_collect, "fit_s": t_fit},
+        "reflection_error": {"learned": err_learned, "thin_cpml_only": err_plain},
+        "ms_per_step": {"thick_cpml": ms_thick, "thin_cpml_only": ms_plain, "thin_learned": ms_learned},
+        "layer_active_at_end": bool(st[0]) if st else None, "monitored_residual": st[1] if st else None,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -586,7 +678,7 @@ def main():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gfb", choices=["gfb", "reference"])
-    ap.add_argument("--workload", default="layered_64x64x32", choices=sorted(WORKLOADS) + ["batch32"])
+    ap.add_argument("--workload", default="layered_64x64x32", choices=sorted(WORKLOADS) + ["batch32"] + sorted(LAYER))
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--fields", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
@@ -603,6 +695,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch32":
         return run_batch(args)
+    if args.workload in LAYER:
+        return run_layer(args)
     return run_gfb(args)
 
 

@@ -7,15 +7,21 @@
 //
 // Network, per node and wavefield (one network per depth class "net"):
 //   x  = 9 channels (u, v, a in the node's face frame, each channel divided
-//        by its scale) x 4 time taps (the states of steps n-1 .. n-4)
-//   h1 = relu(+-W1 x), h2 = relu(W2 h1), y = W3 h2     (no biases)
-//   f(x) = (y(+x) - y(-x)) / 2,  correction = s_c * f(x)
-// Bias-free ReLU layers make y positively homogeneous and the odd
-// combination makes f homogeneous of degree one: scaling the wavefield
-// scales the correction, as for the exact absorbing boundary operator, which
-// is linear.  Weights are BF16; inference runs on the tensor cores (mma.sync
-// m16n8k16, FP32 accumulate); training keeps FP32 master weights, rounds them
-// to BF16 for its forward/backward pass and runs on the CUDA cores.
+//        by its scale) x 4 time taps (the states of steps n-1 .. n-4),
+//        normalised to unit length: xh = x / |x|
+//   h1 = relu(+-W1 xh), h2 = relu(W2 h1), y = W3 h2     (no biases)
+//   sigma_j = softplus((y_j(+xh) + y_j(-xh)) / 2)
+//   correction_j = -(s_c / s_v) sigma_j v_j   (face frame; v_j the velocity
+//                  at the end of the step, the damping taken implicitly)
+// The network predicts damping coefficients of a dashpot on each face axis
+// (a learned, history-dependent generalisation of a viscous absorbing
+// boundary): the correction only takes energy out and adds no stiffness, so
+// the explicit step stays stable; sigma depends on the shape of the recent
+// history, not its size, so the correction is linear in the wavefield's
+// amplitude like the exact absorbing operator.  sigma is capped at m / dt.
+// Weights are BF16; inference runs on the tensor cores (mma.sync m16n8k16,
+// FP32 accumulate); training keeps FP32 master weights, rounds them to BF16
+// for its forward/backward pass and runs on the CUDA cores.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -145,7 +151,7 @@ struct LayerArgs {
     const int* mstep;         // next step index (device counter); this step is mstep - 1
     double dt;
     double* acc;              // [2 parity][2]: work of the correction, boundary kinetic energy
-    double* monitor;          // [0] residual (running mean), [1] steps seen
+    double* monitor;          // [0] residual (running mean), [1] steps seen, [2] steps above threshold in a row
     int* active;              // 1 while the correction is applied
     double threshold;
 };
@@ -186,11 +192,16 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
         pa[0] = 0.0;
         pa[1] = 0.0;
         if (*A.active) {
+            // residual of the step: energy put in by the correction relative
+            // to the kinetic energy of the layer nodes; off for good after 3
+            // steps in a row above the threshold, or at once on a non-finite
+            // value or a residual 100 times the threshold
             const double r = (ekin > 0.0) ? work / ekin : 0.0;
             const double k = A.monitor[1] + 1.0;
-            A.monitor[0] += (r - A.monitor[0]) / fmin(k, 50.0);  // running mean over <= 50 steps
+            A.monitor[0] += (r - A.monitor[0]) / fmin(k, 50.0);  // running mean over <= 50 steps (reported)
             A.monitor[1] = k;
-            if (!(work == work) || (k >= 10.0 && A.monitor[0] > A.threshold)) *A.active = 0;
+            A.monitor[2] = (r > A.threshold) ? A.monitor[2] + 1.0 : 0.0;
+            if (!isfinite(work) || !isfinite(ekin) || A.monitor[2] >= 3.0 || r > 100.0 * A.threshold) *A.active = 0;
         }
     }
     __syncthreads();
@@ -211,9 +222,17 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
             f = smp - b * NF;
             bn = A.bnd[b];
             node_features(bn, f, NF, n, A.u, A.v, A.a, A.ring, A.n_bnd, b, A.sc, x, cur);
+            float nrm = 0.f;
+#pragma unroll
+            for (int q = 0; q < kIn; ++q) nrm += x[q] * x[q];
+            const float inv = nrm > 0.f ? rsqrtf(nrm) : 0.f;
+#pragma unroll
+            for (int q = 0; q < kIn; ++q) x[q] *= inv;
         } else {
 #pragma unroll
             for (int q = 0; q < kIn; ++q) x[q] = 0.f;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) cur[q] = 0.f;
         }
         // half 0 writes k = 0..27, half 1 writes k = 28..55 (zero padding)
 #pragma unroll
@@ -275,19 +294,21 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
             }
         }
         // outputs: lane holds columns c0, c0+1 of rows r0 (y[.][0..1]) and
-        // r0+8 (y[.][2..3]); columns 0..2 are the face-frame correction
-        float outv[4];
+        // r0+8 (y[.][2..3]); columns 0..2 are the face-frame damping logits
+        float sig[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) outv[q] = A.sc[3] * 0.5f * (y[0][q] - y[1][q]);
+        for (int q = 0; q < 4; ++q) {
+            const float fz = 0.5f * (y[0][q] + y[1][q]);
+            sig[q] = fz > 20.f ? fz : log1pf(__expf(fz));  // softplus
+        }
         // gather the three columns of each row in lanes with lane%4 == 0
-        const float o2a = __shfl_down_sync(0xffffffffu, outv[0], 1);  // column 2 of row r0
-        const float o2b = __shfl_down_sync(0xffffffffu, outv[2], 1);  // column 2 of row r0+8
-        // the feature lanes hold cur[] for row = lane/2: bring them to the
-        // output lanes (lane 4r holds rows r and r+8)
+        const float s2a = __shfl_down_sync(0xffffffffu, sig[0], 1);  // column 2 of row r0
+        const float s2b = __shfl_down_sync(0xffffffffu, sig[2], 1);  // column 2 of row r0+8
+        const float gain = A.sc[3] / A.sc[1];
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr) {
             const int orow = r0 + 8 * rr;
-            // cur of row orow lives in lane 2*orow (half 0)
+            // the state of row orow lives in lane 2*orow (half 0)
             float cv[9];
 #pragma unroll
             for (int q = 0; q < 9; ++q) cv[q] = __shfl_sync(0xffffffffu, cur[q], 2 * orow);
@@ -295,23 +316,36 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
             const int oframe = __shfl_sync(0xffffffffu, bn.frame, 2 * orow);
             const int onode = __shfl_sync(0xffffffffu, bn.node, 2 * orow);
             if ((lane & 3) == 0 && osmp >= 0) {
-                const float loc[3] = {rr == 0 ? outv[0] : outv[2], rr == 0 ? outv[1] : outv[3], rr == 0 ? o2a : o2b};
+                const float sl[3] = {rr == 0 ? sig[0] : sig[2], rr == 0 ? sig[1] : sig[3], rr == 0 ? s2a : s2b};
+                const double m = A.mass[onode];
+                const float cap = (float)(m / A.dt);
+                const int of = osmp % NF;
+                float4* dst = reinterpret_cast<float4*>(A.force) + (size_t)onode * NF + of;
+                float4 fo = *dst;
+                const float fe[3] = {fo.x, fo.y, fo.z};
+                const float hdm = (float)(0.5 * A.dt / m);
                 float gc[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int j = 0; j < 3; ++j) gc[frame_axis(oframe, j)] = frame_sign(oframe, j) * loc[j];
-                const int of = osmp % NF;
-                if (on && isfinite(gc[0]) && isfinite(gc[1]) && isfinite(gc[2])) {
-                    float4* dst = reinterpret_cast<float4*>(A.force) + (size_t)onode * NF + of;
-                    float4 fo = *dst;
+                for (int j = 0; j < 3; ++j) {
+                    const int ax = frame_axis(oframe, j);
+                    float dj = gain * sl[j];  // non-finite stays non-finite (the monitor's signal)
+                    if (isfinite(dj)) dj = fminf(dj, cap);
+                    // trapezoidal dashpot: velocity at the end of the step
+                    // estimated from this step's force, the damping taken
+                    // implicitly, so any sigma >= 0 stays stable
+                    const float vbar = cv[3 + ax] + (float)(0.5 * A.dt) * cv[6 + ax] + hdm * fe[ax];
+                    gc[ax] = -dj * vbar / (1.f + dj * hdm);
+                }
+                const bool fin = isfinite(gc[0]) && isfinite(gc[1]) && isfinite(gc[2]);
+                if (on && fin) {
                     fo.x += gc[0];
                     fo.y += gc[1];
                     fo.z += gc[2];
                     *dst = fo;
                 }
                 // work of the correction over the step and kinetic energy
-                const double m = A.mass[onode];
-                work += A.dt * ((double)gc[0] * cv[3] + (double)gc[1] * cv[4] + (double)gc[2] * cv[5]);
-                if (!(isfinite(gc[0]) && isfinite(gc[1]) && isfinite(gc[2]))) work = nan("");
+                work += fin ? A.dt * ((double)gc[0] * cv[3] + (double)gc[1] * cv[4] + (double)gc[2] * cv[5])
+                            : nan("");
                 ekin += 0.5 * m * ((double)cv[3] * cv[3] + (double)cv[4] * cv[4] + (double)cv[5] * cv[5]);
             }
         }
@@ -418,7 +452,7 @@ struct Layer {
     __nv_bfloat16* w = nullptr;
     float sc[4] = {1.f, 1.f, 1.f, 1.f};
     double* acc = nullptr;      // [4]
-    double* monitor = nullptr;  // [2]
+    double* monitor = nullptr;  // [3]
     int* active = nullptr;
     double threshold = 0.0;
     int blocks = 0;
@@ -575,7 +609,7 @@ __global__ void __launch_bounds__(kTB) train_kernel(TrainArgs A) {
     float* dp = hm + kTB * kHid;       // [kTB][64] dz2 (+)
     float* dm = dp + kTB * kHid;       // [kTB][64] dz2 (-)
     float* d1 = dm + kTB * kHid;       // [kTB][64] dz1
-    float* ep = d1 + kTB * kHid;       // [kTB][3] dy (+); dy (-) = -dy (+)
+    float* ep = d1 + kTB * kHid;       // [kTB][3] d loss / d y, the same for both branches
     const int tid = threadIdx.x;
     for (int q = tid; q < kMNet; q += kTB) ts[q] = bf16r(A.wm[q]);
     const int s = blockIdx.x * kTB + tid;
@@ -619,21 +653,27 @@ __global__ void __launch_bounds__(kTB) train_kernel(TrainArgs A) {
             y[br][o] = acc;
         }
     }
+    // c_j = -softplus(f_j) vh_j with f = (y(+x) + y(-x)) / 2 and vh the
+    // newest velocity channels of the normalised features
     double l = 0.0;
-    float e[kOut];
+    float dyv[kOut];
     for (int o = 0; o < kOut; ++o) {
-        e[o] = ok ? 0.5f * (y[0][o] - y[1][o]) - t[o] : 0.f;
-        l += 0.5 * (double)e[o] * e[o];
-        ep[tid * kOut + o] = 0.5f * e[o];  // d loss / d y(+x); d / d y(-x) is its negative
+        const float fz = 0.5f * (y[0][o] + y[1][o]);
+        const float sp = fz > 20.f ? fz : log1pf(expf(fz));
+        const float sgm = 1.f / (1.f + expf(-fz));
+        const float vh = x[3 + o];
+        const float e = ok ? -sp * vh - t[o] : 0.f;
+        l += 0.5 * (double)e * e;
+        dyv[o] = 0.5f * e * (-vh) * sgm;  // d loss / d y(+x) = d loss / d y(-x)
+        ep[tid * kOut + o] = dyv[o];
     }
     // backward to dz2 (+/-) and dz1
     for (int br = 0; br < 2; ++br) {
-        const float sg = br == 0 ? 1.f : -1.f;
         const float* h = br == 0 ? hp : hm;
         float* dz = br == 0 ? dp : dm;
         for (int k = 0; k < kHid; ++k) {
             float g = 0.f;
-            for (int o = 0; o < kOut; ++o) g += w3[o * kHid + k] * sg * 0.5f * e[o];
+            for (int o = 0; o < kOut; ++o) g += w3[o * kHid + k] * dyv[o];
             dz[tid * kHid + k] = h[tid * kHid + k] > 0.f ? g : 0.f;
         }
     }
@@ -661,7 +701,7 @@ __global__ void __launch_bounds__(kTB) train_kernel(TrainArgs A) {
             }
         } else {
             const int qq = q - kM3, o = qq / kHid, k = qq - o * kHid;
-            for (int r = 0; r < kTB; ++r) g += ep[r * kOut + o] * (hp[r * kHid + k] - hm[r * kHid + k]);
+            for (int r = 0; r < kTB; ++r) g += ep[r * kOut + o] * (hp[r * kHid + k] + hm[r * kHid + k]);
         }
         atomicAdd(A.grad + q, g);
     }
@@ -754,10 +794,10 @@ gfb_status gfb_layer_attach(gfb_solver* s, const gfb_layer* layer, const uint16_
         L->sc[q] = scales[q];
     }
     if ((st = L->mem.alloc(&L->acc, 4))) return st;
-    if ((st = L->mem.alloc(&L->monitor, 2))) return st;
+    if ((st = L->mem.alloc(&L->monitor, 3))) return st;
     if ((st = L->mem.alloc(&L->active, 1))) return st;
     LCU(cudaMemset(L->acc, 0, 4 * sizeof(double)));
-    LCU(cudaMemset(L->monitor, 0, 2 * sizeof(double)));
+    LCU(cudaMemset(L->monitor, 0, 3 * sizeof(double)));
     const int one = 1;
     LCU(cudaMemcpy(L->active, &one, sizeof(int), cudaMemcpyHostToDevice));
     L->threshold = threshold;
@@ -1020,6 +1060,33 @@ gfb_status gfb_trainer_fit(gfb_trainer* t, int32_t epochs, int32_t batch, float 
         if (loss) loss[ep] = ep_n ? ep_loss / ep_n : 0.0;
     }
     LCU(cudaStreamSynchronize(t->stream));
+    return GFB_OK;
+}
+
+gfb_status gfb_trainer_evaluate(gfb_trainer* t, double* loss) {
+    using namespace gfb;
+    if (!t || !loss) return set_error(GFB_ERR_INVALID, "NULL argument");
+    LCU(cudaSetDevice(t->device));
+    gfb_status st;
+    if (!t->have_scales && (st = trainer_scales(t))) return st;
+    std::vector<int64_t> cnt(t->n_net);
+    if ((st = gfb_trainer_samples(t, cnt.data()))) return st;
+    double sum = 0.0;
+    long long n = 0;
+    std::vector<int> id(t->max_batch);
+    for (int k = 0; k < t->n_net; ++k)
+        for (long long b0 = 0; b0 < cnt[k]; b0 += t->max_batch) {
+            const int nb = (int)std::min<long long>(t->max_batch, cnt[k] - b0);
+            for (int i = 0; i < nb; ++i) id[i] = (int)(b0 + i);
+            LCU(cudaMemcpyAsync(t->idx, id.data(), nb * 4, cudaMemcpyHostToDevice, t->stream));
+            double l = 0.0;
+            if ((st = trainer_grad(t, k, t->X + (size_t)k * t->capacity * kIn, t->T + (size_t)k * t->capacity * kOut,
+                                   nb, &l)))
+                return st;
+            sum += l;
+            n += nb;
+        }
+    *loss = n ? sum / n : 0.0;
     return GFB_OK;
 }
 

@@ -1524,6 +1524,104 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
     return GFB_OK;
 }
 
+namespace {
+
+// Device arrays of a checkpoint, in order: pointer and byte count.
+std::vector<std::pair<void*, size_t>> checkpoint_arrays(gfb_solver* s) {
+    const size_t es = s->prec == GFB_FP64 ? 8 : 4;
+    const size_t nF = (size_t)s->n_node * s->F;
+    std::vector<std::pair<void*, size_t>> a;
+    a.push_back({s->u, nF * 8});
+    a.push_back({s->v, nF * 8});
+    a.push_back({s->a, nF * es});
+    a.push_back({s->ut, (size_t)s->n_node * s->nfld * 4 * es});
+    if (s->has_cpml && !s->node_pml) {
+        a.push_back({s->pml_mem, (size_t)s->n_pml * s->F * 3 * s->nn * es});
+        a.push_back({s->pml_prev, (size_t)s->n_pml * s->F * s->nn * es});
+    }
+    if (s->node_pml && s->n_pml_node > 0) {
+        a.push_back({s->npml_mem, (size_t)s->n_pml_node * s->F * 3 * es});
+        a.push_back({s->npml_prev, (size_t)s->n_pml_node * s->F * es});
+    }
+    a.push_back({s->d_mstep, (size_t)s->n_model * 4});
+    return a;
+}
+
+struct CheckpointHeader {
+    char magic[8];
+    int64_t bytes;
+    int32_t version, precision, n_field, n_model;
+    int64_t n_node, n_cell, n_pml, n_pml_node;
+    int32_t step, flags;
+};
+
+void checkpoint_header(const gfb_solver* s, int64_t bytes, CheckpointHeader& h) {
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, "GFBCKPT", 8);
+    h.bytes = bytes;
+    h.version = 1;
+    h.precision = s->prec;
+    h.n_field = s->nfld;
+    h.n_model = s->n_model;
+    h.n_node = s->n_node;
+    h.n_cell = s->n_cell;
+    h.n_pml = s->node_pml ? 0 : s->n_pml;
+    h.n_pml_node = s->node_pml ? s->n_pml_node : 0;
+    h.step = s->step;
+    h.flags = s->flags;
+}
+
+}  // namespace
+
+gfb_status gfb_checkpoint_size(gfb_solver* s, int64_t* bytes) {
+    if (!s || !bytes) return fail(GFB_ERR_INVALID, "NULL argument");
+    int64_t b = sizeof(CheckpointHeader);
+    for (auto& a : checkpoint_arrays(s)) b += (int64_t)a.second;
+    *bytes = b;
+    return GFB_OK;
+}
+
+gfb_status gfb_checkpoint_save(gfb_solver* s, void* buf, int64_t bytes) {
+    int64_t need = 0;
+    gfb_status st = gfb_checkpoint_size(s, &need);
+    if (st) return st;
+    if (!buf || bytes < need) return fail(GFB_ERR_INVALID, "checkpoint buffer needs %lld bytes", (long long)need);
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    CheckpointHeader h;
+    checkpoint_header(s, need, h);
+    unsigned char* p = static_cast<unsigned char*>(buf);
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    for (auto& a : checkpoint_arrays(s)) {
+        if ((st = d2h(s, p, a.first, a.second))) return st;
+        p += a.second;
+    }
+    return GFB_OK;
+}
+
+gfb_status gfb_checkpoint_load(gfb_solver* s, const void* buf, int64_t bytes) {
+    int64_t need = 0;
+    gfb_status st = gfb_checkpoint_size(s, &need);
+    if (st) return st;
+    if (!buf || bytes < (int64_t)sizeof(CheckpointHeader)) return fail(GFB_ERR_INVALID, "checkpoint buffer too small");
+    CheckpointHeader h, mine;
+    std::memcpy(&h, buf, sizeof(h));
+    checkpoint_header(s, need, mine);
+    mine.step = h.step;
+    if (std::memcmp(&h, &mine, sizeof(h)) != 0 || bytes < need)
+        return fail(GFB_ERR_INVALID, "checkpoint does not belong to a solver built like this one");
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    const unsigned char* p = static_cast<const unsigned char*>(buf) + sizeof(h);
+    for (auto& a : checkpoint_arrays(s)) {
+        if ((st = h2d(s, a.first, p, a.second))) return st;
+        p += a.second;
+    }
+    s->step = h.step;
+    return GFB_OK;
+}
+
 gfb_status gfb_records_pending(gfb_solver* s, int32_t* n) {
     if (!s || !n) return fail(GFB_ERR_INVALID, "NULL argument");
     std::lock_guard<std::mutex> lk(s->rec_mu);

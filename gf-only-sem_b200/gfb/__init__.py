@@ -138,6 +138,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.gfb_synchronize.argtypes = [C.c_void_p]
     lib.gfb_advance_profiled.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
     lib.gfb_advance_timed.argtypes = [C.c_void_p, C.c_int32, _dp]
+    lib.gfb_checkpoint_size.argtypes = [C.c_void_p, _lp]
+    lib.gfb_checkpoint_save.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    lib.gfb_checkpoint_load.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     lib.gfb_create_batch.argtypes = [C.POINTER(Mesh), C.POINTER(Config), C.POINTER(Source), C.c_int32,
                                      C.POINTER(Model), C.POINTER(C.c_void_p)]
     lib.gfb_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
@@ -153,7 +156,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "gfb_create", "gfb_destroy", "gfb_advance", "gfb_synchronize", "gfb_current_step",
         "gfb_get_state", "gfb_set_state", "gfb_records_pending", "gfb_read_record",
         "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
-        "gfb_create_batch",
+        "gfb_create_batch", "gfb_checkpoint_size", "gfb_checkpoint_save", "gfb_checkpoint_load",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -274,6 +277,19 @@ class Solver:
 
     def advance(self, n_steps: int):
         _check(self.lib.gfb_advance(self.h, int(n_steps)))
+
+    def checkpoint(self) -> bytes:
+        """Exact checkpoint of the time-loop state (gfb_checkpoint_save)."""
+        n = C.c_int64()
+        _check(self.lib.gfb_checkpoint_size(self.h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(self.lib.gfb_checkpoint_save(self.h, buf, n.value))
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Continue from a checkpoint of a solver built from the same inputs."""
+        buf = C.create_string_buffer(data, len(data))
+        _check(self.lib.gfb_checkpoint_load(self.h, buf, len(data)))
 
     def advance_timed(self, n_steps: int) -> float:
         """Advance and return the device milliseconds of the n_steps steps."""

@@ -1,0 +1,341 @@
+"""Learned absorbing layer: thin domain + small networks, trained from replays
+of a thick-C-PML run (C ABI in include/gfb.h, kernels in csrc/gfb_layer.cu).
+
+A model is built twice from the same interior: *thick* with a ``n_thick``-
+element C-PML on the five absorbing faces (x-, x+, y-, y+ and the bottom;
+the top is the free surface) and *thin* with a one-element C-PML.  The thin
+domain's layer nodes get a force correction from one network per node class
+(side or bottom face x depth plane inside the layer cell); the networks are
+trained so that the thin run follows the thick run, which is also the judge
+of the reflection error.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import (FP32, FLAG_RECORD_F32, Solver, _check, _ptr, load_library)
+from . import mesh
+
+N_PARAMS = 6592      # GFB_LAYER_PARAMS
+N_WEIGHTS = 8768     # GFB_LAYER_WEIGHTS
+N_IN, N_HID, N_OUT = 36, 64, 3
+
+
+class LayerDesc(C.Structure):
+    _fields_ = [
+        ("n_node", C.c_int32),
+        ("node", C.POINTER(C.c_int32)),
+        ("frame", C.POINTER(C.c_int8)),
+        ("net", C.POINTER(C.c_uint8)),
+        ("n_net", C.c_int32),
+    ]
+
+
+def _bind(lib):
+    if getattr(lib, "_layer_bound", False):
+        return lib
+    vp, i32, i64, u64, f32p, dp = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_double)
+    lib.gfb_layer_pack.argtypes = [i32, f32p, C.POINTER(C.c_uint16)]
+    lib.gfb_layer_attach.argtypes = [vp, C.POINTER(LayerDesc), C.POINTER(C.c_uint16), f32p, C.c_double]
+    lib.gfb_layer_status.argtypes = [vp, C.POINTER(C.c_int32), dp]
+    lib.gfb_trainer_create.argtypes = [i32, i64, i32, u64, C.POINTER(vp)]
+    lib.gfb_trainer_destroy.argtypes = [vp]
+    lib.gfb_trainer_collect.argtypes = [vp, vp, vp, C.POINTER(C.c_int32), C.POINTER(LayerDesc), i32, i32, i32]
+    lib.gfb_trainer_samples.argtypes = [vp, C.POINTER(C.c_int64)]
+    lib.gfb_trainer_set_scales.argtypes = [vp, f32p]
+    lib.gfb_trainer_fit.argtypes = [vp, i32, i32, C.c_float, u64, dp]
+    lib.gfb_trainer_gradient.argtypes = [vp, i32, i32, f32p, f32p, f32p, dp]
+    lib.gfb_trainer_get_params.argtypes = [vp, f32p, f32p]
+    lib.gfb_trainer_set_params.argtypes = [vp, f32p]
+    lib.gfb_trainer_evaluate.argtypes = [vp, dp]
+    for n in ("gfb_layer_pack", "gfb_layer_attach", "gfb_layer_status", "gfb_trainer_create", "gfb_trainer_destroy",
+              "gfb_trainer_collect", "gfb_trainer_samples", "gfb_trainer_set_scales", "gfb_trainer_fit",
+              "gfb_trainer_gradient", "gfb_trainer_get_params", "gfb_trainer_set_params", "gfb_trainer_evaluate"):
+        getattr(lib, n).restype = C.c_int
+    lib._layer_bound = True
+    return lib
+
+
+# ---------------------------------------------------------------------------
+# models
+# ---------------------------------------------------------------------------
+
+@dataclass
+class PairSpec:
+    """Interior of ni x nj x nk cells of size d; layered material; a point
+    source in the interior (interior coordinates); Ricker f0."""
+    ni: int
+    nj: int
+    nk: int
+    d: float
+    seed: int
+    src: tuple
+    f0: float = 2.0
+    nsteps: int = 1000
+    stride: int = 10
+    n_thick: int = 10
+    n_thin: int = 1
+    dt: Optional[float] = None
+
+
+def build_domain(p: PairSpec, n_layer: int, dt: Optional[float] = None, with_cpml: bool = True) -> dict:
+    """The model with an n_layer-element C-PML (or the legacy damping layer)
+    on the absorbing faces; interior cell (0, 0, 0) starts at
+    (n_layer d, n_layer d, 0)."""
+    faces = {"xmin": n_layer, "xmax": n_layer, "ymin": n_layer, "ymax": n_layer, "zmax": n_layer}
+    spec = mesh.MeshSpec(nx=p.ni + 2 * n_layer, ny=p.nj + 2 * n_layer, nz=p.nk + n_layer, dx=p.d, dy=p.d, dz=p.d,
+                         order=4, pml=faces)
+    mat = mesh.seeded_layers(p.seed, p.nk * p.d)
+    src = np.array([p.src[0] + n_layer * p.d, p.src[1] + n_layer * p.d, p.src[2]])
+    prob = mesh.build_problem(spec, mat, src, dt=dt, nsteps=p.nsteps, snapshot_stride=p.stride,
+                              record_depth_max_m=p.d, f0=p.f0, with_cpml=with_cpml)
+    prob["n_layer"] = n_layer
+    return prob
+
+
+def build_pair(p: PairSpec):
+    """(thin, thick) problems with one time step (the smaller of the two
+    CFL steps) and the thin->thick node map."""
+    thick = build_domain(p, p.n_thick, p.dt)
+    thin = build_domain(p, p.n_thin, thick["dt"])
+    return thin, thick, node_map(thin, thick, (p.n_thick - p.n_thin) * p.d)
+
+
+def _node_coords(prob):
+    nn = prob["ngll"] ** 3
+    c = np.asarray(prob["coords"]).reshape(-1, 3)
+    ib = np.asarray(prob["ibool"]).ravel()
+    out = np.empty((prob["n_node"], 3))
+    out[ib] = c
+    return out
+
+
+def node_map(thin: dict, thick: dict, shift: float) -> np.ndarray:
+    """thick node id of every thin node (positions equal after shifting the
+    thin mesh by `shift` in x and y)."""
+    a = _node_coords(thin) + np.array([shift, shift, 0.0])
+    b = _node_coords(thick)
+    scale = 1e-6 * max(np.ptp(b[:, 0]), 1.0)
+    qa = np.rint(a / scale).astype(np.int64)
+    qb = np.rint(b / scale).astype(np.int64)
+    ka = (qa[:, 0] * 1_000_003 + qa[:, 1]) * 1_000_033 + qa[:, 2]
+    kb = (qb[:, 0] * 1_000_003 + qb[:, 1]) * 1_000_033 + qb[:, 2]
+    order = np.argsort(kb)
+    pos = np.searchsorted(kb[order], ka)
+    pos = np.clip(pos, 0, kb.size - 1)
+    hit = order[pos]
+    if not np.all(np.all(qb[hit] == qa, axis=1)):
+        raise ValueError("thin mesh nodes not found in the thick mesh")
+    return hit.astype(np.int32)
+
+
+# ---------------------------------------------------------------------------
+# layer nodes: class (network), face frame
+# ---------------------------------------------------------------------------
+
+FACES = ("xmin", "xmax", "ymin", "ymax", "zmax")
+# local axes (1-based global axis, signed; local 0 = outward normal)
+FRAMES = {"xmin": (-1, 2, 3), "xmax": (1, 2, 3), "ymin": (-2, 1, 3), "ymax": (2, 1, 3), "zmax": (3, 1, 2)}
+
+
+def layer_nodes(prob: dict, planes=None):
+    """Nodes of the one-element layer cells of a thin domain: node ids, face
+    frames and network index = (0 side face, 1 bottom) * 5 + depth plane
+    (0 at the interior interface, 4 at the truncation surface).  A node in
+    the layer of several faces takes the face it is deepest in.  ``planes``
+    keeps only those depth planes (default: the truncation surface, where
+    the missing outer domain acts on the thin one)."""
+    d = prob["spec"].dx
+    L = prob["n_layer"]
+    ng = prob["ngll"]
+    gll = mesh.gll_points(ng - 1)
+    pos = (gll + 1.0) / 2.0  # fraction across an element
+    X = _node_coords(prob)
+    b = prob["bounds"]
+    # distance into each face's layer, in elements (0 at the interface)
+    inward = {
+        "xmin": (b["xmin"] + L * d - X[:, 0]) / d,
+        "xmax": (X[:, 0] - (b["xmax"] - L * d)) / d,
+        "ymin": (b["ymin"] + L * d - X[:, 1]) / d,
+        "ymax": (X[:, 1] - (b["ymax"] - L * d)) / d,
+        "zmax": (X[:, 2] - (b["zmax"] - L * d)) / d,
+    }
+    best = np.full(X.shape[0], -1.0)
+    face = np.full(X.shape[0], -1)
+    for k, f in enumerate(FACES):
+        dist = inward[f]
+        take = (dist > -1e-9) & (dist > best + 1e-9)
+        best[take] = dist[take]
+        face[take] = k
+    sel = np.nonzero(face >= 0)[0]
+    plane = np.abs(best[sel][:, None] - pos[None, :]).argmin(axis=1)
+    keep = np.isin(plane, list(planes if planes is not None else (ng - 1,)))
+    sel, plane = sel[keep], plane[keep]
+    fr = np.array([FRAMES[FACES[k]] for k in face[sel]], dtype=np.int8)
+    net = np.where(face[sel] == 4, 1, 0) * ng + plane
+    return sel.astype(np.int32), fr, net.astype(np.uint8), 2 * ng
+
+
+class Layer:
+    """Layer description passed through the C ABI."""
+
+    def __init__(self, prob: dict, planes=None):
+        self.node, self.frame, self.net, self.n_net = layer_nodes(prob, planes)
+        self.desc = LayerDesc()
+        self.desc.n_node = int(self.node.size)
+        self.desc.node = _ptr(self.node, C.c_int32)
+        self.desc.frame = self.frame.ctypes.data_as(C.POINTER(C.c_int8))
+        self.desc.net = self.net.ctypes.data_as(C.POINTER(C.c_uint8))
+        self.desc.n_net = int(self.n_net)
+
+
+# ---------------------------------------------------------------------------
+# training
+# ---------------------------------------------------------------------------
+
+class Trainer:
+    def __init__(self, n_net: int, capacity: int, device: int = 0, seed: int = 0):
+        self.lib = _bind(load_library())
+        self.n_net = n_net
+        h = C.c_void_p()
+        _check(self.lib.gfb_trainer_create(n_net, int(capacity), device, int(seed), C.byref(h)))
+        self.h = h
+
+    def collect(self, thin: Solver, thick: Solver, thin_to_thick: np.ndarray, layer: Layer, n_steps: int,
+                sample_stride: int = 1, node_stride: int = 1):
+        m = np.ascontiguousarray(thin_to_thick, dtype=np.int32)
+        _check(self.lib.gfb_trainer_collect(self.h, thin.h, thick.h, _ptr(m, C.c_int32), C.byref(layer.desc),
+                                            int(n_steps), int(sample_stride), int(node_stride)))
+
+    def samples(self) -> np.ndarray:
+        c = np.zeros(self.n_net, dtype=np.int64)
+        _check(self.lib.gfb_trainer_samples(self.h, c.ctypes.data_as(C.POINTER(C.c_int64))))
+        return c
+
+    def set_scales(self, scales):
+        s = np.ascontiguousarray(scales, dtype=np.float32)
+        _check(self.lib.gfb_trainer_set_scales(self.h, _ptr(s, C.c_float)))
+
+    def evaluate(self) -> float:
+        """Mean loss over every collected sample at the current parameters."""
+        l = C.c_double()
+        _check(self.lib.gfb_trainer_evaluate(self.h, C.byref(l)))
+        return l.value
+
+    def baseline_loss(self) -> float:
+        """Mean loss of predicting zero on the collected samples (with the
+        scales the fit uses): the yardstick of the fitted loss."""
+        p, _ = self.params()
+        self.set_params(np.zeros_like(p))
+        l = self.evaluate()
+        self.set_params(p)
+        return l
+
+    def fit(self, epochs: int, batch: int = 2048, lr: float = 1e-3, seed: int = 0):
+        loss = np.zeros(max(epochs, 1))
+        _check(self.lib.gfb_trainer_fit(self.h, int(epochs), int(batch), C.c_float(lr), int(seed),
+                                        _ptr(loss, C.c_double)))
+        return loss[:epochs]
+
+    def gradient(self, net: int, x: np.ndarray, y: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(N_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        _check(self.lib.gfb_trainer_gradient(self.h, int(net), int(x.shape[0]), _ptr(x, C.c_float),
+                                             _ptr(y, C.c_float), _ptr(g, C.c_float), C.byref(loss)))
+        return g, loss.value
+
+    def params(self):
+        p = np.zeros((self.n_net, N_PARAMS), dtype=np.float32)
+        s = np.zeros(4, dtype=np.float32)
+        _check(self.lib.gfb_trainer_get_params(self.h, _ptr(p, C.c_float), _ptr(s, C.c_float)))
+        return p, s
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self.lib.gfb_trainer_set_params(self.h, _ptr(p, C.c_float)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gfb_trainer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pack(params: np.ndarray) -> np.ndarray:
+    lib = _bind(load_library())
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    n_net = p.shape[0]
+    w = np.zeros(n_net * N_WEIGHTS, dtype=np.uint16)
+    _check(lib.gfb_layer_pack(n_net, _ptr(p, C.c_float), w.ctypes.data_as(C.POINTER(C.c_uint16))))
+    return w
+
+
+def attach(solver: Solver, layer: Layer, params: np.ndarray, scales: np.ndarray, threshold: float = 0.05):
+    lib = _bind(load_library())
+    w = pack(params)
+    s = np.ascontiguousarray(scales, dtype=np.float32)
+    _check(lib.gfb_layer_attach(solver.h, C.byref(layer.desc), w.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                _ptr(s, C.c_float), float(threshold)))
+    solver._layer_keep = (layer, w, s)
+
+
+def status(solver: Solver):
+    lib = _bind(load_library())
+    a = C.c_int32()
+    r = C.c_double()
+    _check(lib.gfb_layer_status(solver.h, C.byref(a), C.byref(r)))
+    return bool(a.value), r.value
+
+
+def collect_pair(trainer: Trainer, p: PairSpec, dirs=(0, 1, 2), n_steps: Optional[int] = None,
+                 sample_stride: int = 2, node_stride: int = 1, device: int = 0):
+    """Replay one thin/thick pair into the trainer's data set."""
+    thin, thick, m = build_pair(p)
+    layer = Layer(thin)
+    st = Solver(thin, dirs=dirs, precision=FP32, device=device, record=False)
+    sk = Solver(thick, dirs=dirs, precision=FP32, device=device, record=False)
+    trainer.collect(st, sk, m, layer, n_steps or p.nsteps, sample_stride, node_stride)
+    st.close()
+    sk.close()
+
+
+# ---------------------------------------------------------------------------
+# evaluation against the thick-C-PML judge
+# ---------------------------------------------------------------------------
+
+def surface_records(prob: dict, snaps: dict, shift: float):
+    """Recorded displacement of the interior surface cells, keyed by cell
+    centre (so thin and thick runs can be matched)."""
+    nn = prob["ngll"] ** 3
+    rec = np.asarray(prob["recording"]["rec_cell_local"])
+    c = np.asarray(prob["coords"]).reshape(prob["n_cell"], nn, 3)[rec].mean(axis=1) + np.array([shift, shift, 0.0])
+    key = np.rint(c / 1e-3).astype(np.int64)
+    return key, np.asarray(snaps["u"])  # [n_snap][n_rec][nn][3]
+
+
+def reflection_error(thin: dict, thin_snaps: dict, thick: dict, thick_snaps: dict, shift: float) -> float:
+    """||u_thin - u_thick|| / ||u_thick|| over every snapshot of the thin
+    domain's recorded interior surface cells."""
+    ka, ua = surface_records(thin, thin_snaps, shift)
+    kb, ub = surface_records(thick, thick_snaps, 0.0)
+    idx = {tuple(k): i for i, k in enumerate(kb)}
+    sel = [i for i, k in enumerate(ka) if tuple(k) in idx]
+    if not sel:
+        raise ValueError("no common recording cells")
+    pick = [idx[tuple(ka[i])] for i in sel]
+    a = ua[:, sel]
+    b = ub[:, pick]
+    n = min(a.shape[0], b.shape[0])
+    return float(np.linalg.norm(a[:n] - b[:n]) / max(np.linalg.norm(b[:n]), 1e-300))

@@ -248,6 +248,19 @@ gfb_status gfb_get_state(gfb_solver* solver, int32_t field, double* u, double* v
 gfb_status gfb_set_state(gfb_solver* solver, int32_t field, int32_t step, const double* u,
                          const double* v, const double* a);
 
+/*
+ * Exact checkpoint of the time loop: u, v, a, the predicted displacement,
+ * the C-PML memory and previous fields (per cell or per node) and the step
+ * counters, in the device layout.  The reference's restart file keeps u, v,
+ * a only (restart.cpp:120-152), so its resume restarts C-PML memory from
+ * zero; loading a checkpoint continues bit for bit.  A checkpoint loads
+ * into a solver built from the same inputs and flags (checked); snapshots
+ * pending in the ring and a learned layer's history are not part of it.
+ */
+gfb_status gfb_checkpoint_size(gfb_solver* solver, int64_t* bytes);
+gfb_status gfb_checkpoint_save(gfb_solver* solver, void* buffer, int64_t bytes);
+gfb_status gfb_checkpoint_load(gfb_solver* solver, const void* buffer, int64_t bytes);
+
 /* Number of snapshots waiting to be read.  gfb_records_pending and
  * gfb_read_record may be called from another host thread while
  * gfb_advance runs (a writer thread draining records); all other calls on a
@@ -318,18 +331,21 @@ gfb_status gfb_element_residual_noalloc(int32_t n_elem, const double* dxi_dx, co
  * A thin domain (the model plus a one-element C-PML layer) gets a force
  * correction at the nodes of its layer cells from a small network per node
  * class ("net"): inputs are u, v, a of the node (in the node's face frame,
- * each channel divided by its scale) over the last 4 steps, 36 values;
- * hidden layers relu(+-W1 x) and relu(W2 h) of 64; output W3 h in the face
- * frame; correction = s_c (f(x) - f(-x)) / 2 (bias-free, so the correction
- * scales with the wavefield).  Weights are BF16 and inference runs on the
+ * each channel divided by its scale) over the last 4 steps, 36 values,
+ * normalised to unit length (xh); hidden layers relu(+-W1 xh) and
+ * relu(W2 h) of 64; output W3 h; damping sigma_j = softplus of the mean of
+ * the +xh and -xh outputs; correction_j = -(s_c / s_v) sigma_j v_j in the
+ * face frame (a learned dashpot, at most m/dt), which only takes energy out
+ * and scales with the wavefield.  Weights are BF16 and inference runs on the
  * tensor cores with FP32 accumulation, between the element and node phases
  * of every step.  The networks are trained on the GPU from replays of a
  * thick-C-PML run of the enlarged domain: the thick run's state is copied
  * into the thin solver each step and the target is m (a_thick - a_thin).
- * A monitor keeps the running mean over recent steps of (work done by the
- * correction) / (kinetic energy of the layer nodes); above the threshold,
- * or on a non-finite value, the correction is switched off for good and the
- * layer is plain one-element C-PML (the fallback).
+ * A monitor tracks, per step, the work done by the correction relative to
+ * the kinetic energy of the layer nodes: three steps in a row above the
+ * threshold, a value 100 times the threshold, or a non-finite value switch
+ * the correction off for good and the layer is plain one-element C-PML (the
+ * fallback).
  * ------------------------------------------------------------------------ */
 #define GFB_LAYER_NIN 36
 #define GFB_LAYER_NHID 64
@@ -391,6 +407,9 @@ gfb_status gfb_trainer_set_scales(gfb_trainer* trainer, const float* scales);
  * targets); loss[epochs] receives the mean loss of each epoch. */
 gfb_status gfb_trainer_fit(gfb_trainer* trainer, int32_t epochs, int32_t batch, float lr, uint64_t seed,
                            double* loss);
+
+/* Mean loss over every collected sample at the current parameters. */
+gfb_status gfb_trainer_evaluate(gfb_trainer* trainer, double* loss);
 
 /* Gradient of the summed loss over n given samples (raw face-frame features
  * [n][36], targets [n][3]) for network `net` at the current parameters. */

@@ -99,3 +99,32 @@ def test_resume_after_set_state_with_graph(models):
     res.advance(30)
     for x, y in zip(res.state(0), full.state(0)):
         np.testing.assert_allclose(x, y, rtol=0, atol=1e-6 * np.abs(y).max())
+
+
+@pytest.mark.parametrize("prec,flags", [(gfb.FP32, 0), (gfb.FP32, gfb.FLAG_CELL_PML), (gfb.FP64, 0)])
+def test_checkpoint_resume_is_exact_with_cpml(models, prec, flags):
+    """gfb_checkpoint_save/load carry the C-PML memory, so a resumed run
+    continues bit for bit (the reference's restart keeps u, v, a only)."""
+    p = models[0]
+    a = gfb.Solver(p, dirs=[0, 2], precision=prec, flags=flags)
+    a.advance(30)
+    ck = a.checkpoint()
+    a.drain()
+    a.advance(45)
+    ref = a.drain()
+    sa = [a.state(f) for f in range(2)]
+    b = gfb.Solver(p, dirs=[0, 2], precision=prec, flags=flags)
+    b.restore(ck)
+    assert b.step == 30
+    b.advance(45)
+    got = b.drain()
+    for f in range(2):
+        np.testing.assert_array_equal(got[f]["steps"], ref[f]["steps"])
+        for name in ("strain", "u", "v", "a"):
+            np.testing.assert_array_equal(got[f][name], ref[f][name])
+        for x, y in zip(b.state(f), sa[f]):
+            np.testing.assert_array_equal(x, y)
+    # a checkpoint of another configuration is refused
+    c = gfb.Solver(p, dirs=[0], precision=prec, flags=flags)
+    with pytest.raises(gfb.GfbError):
+        c.restore(ck)
