@@ -260,8 +260,13 @@ def run_layer(args):
     judge, ms_thick, _ = run(thick, False)
     plain, ms_plain, _ = run(thin, False)
     learned, ms_learned, st = run(thin, True)
+    trained = params
+    params = params * 0.0  # the same layer untrained: constant damping softplus(0) on every axis
+    untrained, _, _ = run(thin, True)
+    params = trained
     err_plain = [gl.reflection_error(thin, plain[f], thick, judge[f], shift) for f in range(3)]
     err_learned = [gl.reflection_error(thin, learned[f], thick, judge[f], shift) for f in range(3)]
+    err_untrained = [gl.reflection_error(thin, untrained[f], thick, judge[f], shift) for f in range(3)]
     value = float(np.sqrt(np.mean(np.square(err_learned))))
     line = {
         "metric": "reflection error of a learned 1-element absorbing layer vs a 10-element C-PML "
@@ -275,7 +280,8 @@ def run_layer(args):
                    "loss_zero_prediction": base, "loss_first_epoch": float(loss[0]) if len(loss) else None,
                    "loss_last_epoch": float(loss[-1]) if len(loss) else None,
                    "collect_s": t_collect, "fit_s": t_fit},
-        "reflection_error": {"learned": err_learned, "thin_cpml_only": err_plain},
+        "reflection_error": {"learned": err_learned, "thin_cpml_only": err_plain,
+                             "untrained_network_constant_damping": err_untrained},
         "ms_per_step": {"thick_cpml": ms_thick, "thin_cpml_only": ms_plain, "thin_learned": ms_learned},
         "layer_active_at_end": bool(st[0]) if st else None, "monitored_residual": st[1] if st else None,
     }
@@ -617,6 +623,7 @@ def run_gfb(args):
     # set-up), K steps, every snapshot read back to host, destroy
     t0 = time.perf_counter()
     s2 = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8, flags=flags)
+    t_create = time.perf_counter() - t0
     up = s2.info()["upload_bytes"]
     s2.advance(args.steps)
     rec = s2.drain()
@@ -657,6 +664,7 @@ def run_gfb(args):
                           "algorithmic_bytes_per_step": nb},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": up / args.steps,
                 "d2h_bytes_per_step": rec_bytes / args.steps,
+                "create_s": t_create, "total_s": e2e_t,
                 "note": "gfb_create from host arrays + K steps + all snapshots read to host + destroy"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

@@ -216,3 +216,47 @@ def gl_split(p):
     w2 = p[64 * 36: 64 * 36 + 64 * 64].reshape(64, 64)
     w3 = p[64 * 36 + 64 * 64:].reshape(3, 64)
     return w1, w2, w3
+
+
+def test_trained_layer_reduces_reflection_against_thick_cpml():
+    """End to end on small models: collect replays of two seeded pairs, fit,
+    then the reflection error of the thin domain (one-element C-PML) with the
+    trained layer against the 10-element C-PML judge, on a held-out model,
+    is well below that of the same thin domain without the layer."""
+    def pair(seed, steps):
+        r = np.random.default_rng(seed)
+        return gl.PairSpec(ni=6, nj=6, nk=4, d=500.0, seed=seed, f0=float(r.uniform(0.8, 1.2)),
+                           src=(float(r.uniform(1.5, 4.5) * 500), float(r.uniform(1.5, 4.5) * 500),
+                                float(r.uniform(1.0, 2.5) * 500)), nsteps=steps)
+    p0 = pair(11, 10)
+    n_net = gl.Layer(gl.build_domain(p0, 1)).n_net
+    tr = gl.Trainer(n_net=n_net, capacity=2_000_000, seed=1)
+    for k in range(2):
+        gl.collect_pair(tr, pair(20 + k, 400), sample_stride=3, node_stride=2)
+    assert tr.samples().sum() > 0
+    base = tr.baseline_loss()
+    loss = tr.fit(8, batch=2048, lr=1e-3, seed=2)
+    assert loss[-1] < base
+    params, scales = tr.params()
+    tr.close()
+    p = pair(99, 500)
+    thin, thick, _ = gl.build_pair(p)
+    shift = (p.n_thick - p.n_thin) * p.d
+
+    def run(prob, learned):
+        s = gfb.Solver(prob, dirs=[0], precision=gfb.FP32, record_slots=64)
+        if learned:
+            gl.attach(s, gl.Layer(prob), params, scales, threshold=0.05)
+        s.advance(p.nsteps)
+        out = s.drain()[0]
+        st = gl.status(s) if learned else None
+        s.close()
+        return out, st
+
+    judge, _ = run(thick, False)
+    plain, _ = run(thin, False)
+    learned, st = run(thin, True)
+    assert st[0]  # still active: no fallback was needed
+    e_plain = gl.reflection_error(thin, plain, thick, judge, shift)
+    e_learned = gl.reflection_error(thin, learned, thick, judge, shift)
+    assert e_learned < 0.7 * e_plain, (e_learned, e_plain)
