@@ -72,7 +72,7 @@ BATCH = dict(n_model=32, seed=4, d=250.0, pml=4, nmin=(16, 16, 8), nmax=(48, 48,
 # model (interior 94 x 94 x 47), judged against the same interior with a
 # 10-element C-PML; networks trained on replays of small seeded models
 LAYER = {
-    "layer96": dict(ni=94, nk=47, d=250.0, seed=2, steps=2000, stride=10,
+    "layer96": dict(ni=94, nk=47, d=250.0, seed=2, steps=2000, stride=50,
                     train_pairs=24, train_ni=10, train_nk=6, train_steps=700, epochs=30),
     "layer24": dict(ni=22, nk=11, d=250.0, seed=2, steps=900, stride=10,
                     train_pairs=6, train_ni=8, train_nk=5, train_steps=500, epochs=15),
@@ -212,11 +212,11 @@ def run_layer(args):
     rng = np.random.default_rng(w["seed"])
     d = w["d"]
 
-    def pair(seed, ni, nk, steps):
+    def pair(seed, ni, nk, steps, stride=10):
         r = np.random.default_rng(seed)
         return gl.PairSpec(ni=ni, nj=ni, nk=nk, d=d, seed=seed, f0=float(r.uniform(1.5, 2.5)),
                            src=(float(r.uniform(1.5, ni - 1.5) * d), float(r.uniform(1.5, ni - 1.5) * d),
-                                float(r.uniform(1.0, nk - 1.5) * d)), nsteps=steps)
+                                float(r.uniform(1.0, nk - 1.5) * d)), nsteps=steps, stride=stride)
 
     t0 = time.perf_counter()
     p0 = pair(1, w["train_ni"], w["train_nk"], 10)
@@ -234,8 +234,10 @@ def run_layer(args):
     samples = int(tr.samples().sum())
     tr.close()
 
-    p = pair(w["seed"], w["ni"], w["nk"], w["steps"])
-    thin, thick, _ = gl.build_pair(p)
+    # the evaluation model: the thick judge first, then (with the thick
+    # problem freed) the thin domain at the same time step
+    p = pair(w["seed"], w["ni"], w["nk"], w["steps"], w["stride"])
+    thick = gl.build_domain(p, p.n_thick)
     shift = (p.n_thick - p.n_thin) * d
 
     def run(prob, learned):
@@ -243,30 +245,47 @@ def run_layer(args):
                        flags=gfb.FLAG_RECORD_F32)
         if learned:
             gl.attach(s, gl.Layer(prob), params, scales, threshold=0.05)
-        consumer_snaps = []
+        # only the recorded displacement is kept (float32): the judge's
+        # quantity, and small enough for 96 x 96 surface cells
+        import ctypes as C
+
+        us = {f: [] for f in range(3)}
+        step = C.c_int32()
+        null = C.cast(None, C.POINTER(C.c_double))
+
+        def read_all():
+            while s.pending() > 0:
+                for f in range(3):
+                    u = np.zeros((s.n_rec, s.nn, 3))
+                    gfb._check(s.lib.gfb_read_record(s.h, f, C.byref(step), null,
+                                                     u.ctypes.data_as(C.POINTER(C.c_double)), null, null, 0))
+                    us[f].append(u.astype(np.float32))
+
         ms = 0.0
         done = 0
         while done < w["steps"]:
             k = min(200, w["steps"] - done)
             ms += s.advance_timed(k)
-            consumer_snaps.append(s.drain())
+            read_all()
             done += k
         st = gl.status(s) if learned else None
         s.close()
-        snaps = {f: {key: np.concatenate([np.asarray(c[f][key]) for c in consumer_snaps]) for key in
-                     ("steps", "strain", "u", "v", "a")} for f in range(3)}
+        snaps = {f: {"u": np.stack(us[f])} for f in range(3)}
         return snaps, ms / w["steps"], st
 
     judge, ms_thick, _ = run(thick, False)
+    thick_keys, thick_cells, dt = gl.surface_keys(thick), thick["n_cell"], thick["dt"]
+    del thick
+    thin = gl.build_domain(p, p.n_thin, dt)
     plain, ms_plain, _ = run(thin, False)
     learned, ms_learned, st = run(thin, True)
     trained = params
     params = params * 0.0  # the same layer untrained: constant damping softplus(0) on every axis
     untrained, _, _ = run(thin, True)
     params = trained
-    err_plain = [gl.reflection_error(thin, plain[f], thick, judge[f], shift) for f in range(3)]
-    err_learned = [gl.reflection_error(thin, learned[f], thick, judge[f], shift) for f in range(3)]
-    err_untrained = [gl.reflection_error(thin, untrained[f], thick, judge[f], shift) for f in range(3)]
+    err_plain = [gl.reflection_error(thin, plain[f], thick_keys, judge[f], shift) for f in range(3)]
+    err_learned = [gl.reflection_error(thin, learned[f], thick_keys, judge[f], shift) for f in range(3)]
+    err_untrained = [gl.reflection_error(thin, untrained[f], thick_keys, judge[f], shift) for f in range(3)]
     value = float(np.sqrt(np.mean(np.square(err_learned))))
     line = {
         "metric": "reflection error of a learned 1-element absorbing layer vs a 10-element C-PML "
@@ -274,8 +293,8 @@ def run_layer(args):
         "value": value, "unit": "rel L2", "n_gpus": 1, "steps": w["steps"], "warmup": 0,
         "ms_per_step": ms_learned, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 solver, bf16 network weights", "data": "synthetic",
-        "config": {"workload": args.workload, "thin_cells": thin["n_cell"], "thick_cells": thick["n_cell"],
-                   "fewer_elements": 1.0 - thin["n_cell"] / thick["n_cell"],
+        "config": {"workload": args.workload, "thin_cells": thin["n_cell"], "thick_cells": thick_cells,
+                   "fewer_elements": 1.0 - thin["n_cell"] / thick_cells,
                    "train_pairs": w["train_pairs"], "train_samples": samples, "epochs": w["epochs"],
                    "loss_zero_prediction": base, "loss_first_epoch": float(loss[0]) if len(loss) else None,
                    "loss_last_epoch": float(loss[-1]) if len(loss) else None,

@@ -1187,4 +1187,32 @@ __global__ void record_kernel(RecArgs<Real, Out> A) {
     }
 }
 
+
+// Recording nodes merged across the recording cells that share them (the
+// strain Green's-function extraction of postprocess/cpp/main.cpp:300-425):
+// strain mass-weighted, sum(m_p e_p) / sum(m_p) over the node's (cell, point)
+// occurrences; u, v, a averaged.  One thread per (wavefield, node, value),
+// reading the snapshot's cell-point records (out[field][rec][NN][15]) and
+// writing merged[field][node][15] behind them in the same slot.
+template <typename Out>
+__global__ void merge_nodes_kernel(int n_field, int n_unique, long long per_field, const int* ptr, const int* occ,
+                                   const double* w, Out* slot) {
+    const long long total = (long long)n_field * n_unique * 15;
+    Out* merged = slot + (size_t)n_field * per_field;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t % 15);
+        const long long fn = t / 15;
+        const int node = (int)(fn % n_unique), f = (int)(fn / n_unique);
+        const Out* src = slot + (size_t)f * per_field;
+        double acc = 0.0, ws = 0.0;
+        for (int k = ptr[node]; k < ptr[node + 1]; ++k) {
+            const double wk = c < 6 ? w[k] : 1.0;
+            acc += wk * (double)src[(size_t)occ[k] * 15 + c];
+            ws += wk;
+        }
+        merged[((size_t)f * n_unique + node) * 15 + c] = (Out)(ws > 0.0 ? acc / ws : 0.0);
+    }
+}
+
 }  // namespace gfb

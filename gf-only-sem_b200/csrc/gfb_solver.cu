@@ -168,6 +168,12 @@ struct gfb_solver {
     int *src_head = nullptr, *src_next = nullptr;
     void* src_w = nullptr;
     int* rec_cell = nullptr;
+    // recording nodes merged across cells: unique node ids (ascending), CSR
+    // of their (recording cell, point) occurrences and mass weights
+    int n_unique = 0;
+    std::vector<int64_t> rec_node_ids;
+    int *gf_ptr = nullptr, *gf_occ = nullptr;
+    double* gf_w = nullptr;
     // models sharing the solver (one for gfb_create): constants, step
     // counters and source time functions on the device, so that a step
     // captured in a CUDA graph replays correctly
@@ -620,7 +626,12 @@ gfb_status launch_predict(gfb_solver* s) {
     return s->prec == GFB_FP64 ? launch_predict_t<double>(s) : launch_predict_t<float>(s);
 }
 
-size_t snapshot_values(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
+// A snapshot: the recording cells' records [field][rec][NN][15], then the
+// same values merged per recording node [field][node][15].
+size_t snapshot_cell_values(const gfb_solver* s) { return (size_t)s->nfld * s->n_rec * s->nn * 15; }
+size_t snapshot_values(const gfb_solver* s) {
+    return snapshot_cell_values(s) + (size_t)s->nfld * s->n_unique * 15;
+}
 size_t snapshot_bytes(const gfb_solver* s) { return snapshot_values(s) * (s->rec_f32 ? 4 : 8); }
 
 // Convert n snapshot values starting at value `off` of a raw snapshot
@@ -653,7 +664,7 @@ gfb_status spill(gfb_solver* s, Snapshot& snap) {
 // w J/rho A_k (k = 1..5, accumulated in FP64 in cell order), and for each
 // axis the convolution coefficients of the cells where that axis acts.
 // Returns false (per-cell form) if two cells disagree on an axis's
-// coefficients at a shared node.  slot[g] numbers the C-PML nodes in
+// coefficients at a shared node (beyond 1e-6 relative).  slot[g] numbers the C-PML nodes in
 // increasing node order; coef is [slot][14].
 bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w, std::vector<int>& slot,
                    std::vector<double>& coef) {
@@ -694,7 +705,11 @@ bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<dou
                 } else {
                     for (int t = 0; t < 3; ++t) {
                         const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
-                        if (std::abs(a0 - a1) > 1e-9 * std::max(std::abs(a0), std::abs(a1))) return false;
+                        // the cells' coefficients at a node come from the same position
+                        // through different cell maps: equal up to rounding (seen up to
+                        // ~1e-9 relative on deformed meshes); different profiles differ
+                        // at O(1)
+                        if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) return false;
                     }
                 }
             }
@@ -735,23 +750,50 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     const int ng = s->ng, nn = s->nn;
     const long long n_cell = s->n_cell;
     gfb_status st;
-    // C-PML at global nodes (FP32 path) when the cells agree at shared nodes;
-    // its nodes become device nodes [0, n_pml_node), the others follow, both
-    // in increasing node order
+    // C-PML at global nodes (FP32 path) when the cells agree at shared nodes.
+    // Device node order: the node-form C-PML nodes first (so they are device
+    // nodes [0, n_pml_node)), then the others; within each, nodes in the
+    // order cells (in mesh order) first touch them, so the nodes of a cell
+    // and of its neighbours sit close in memory whatever the input
+    // numbering (the reference's coordinate sort scatters them on deformed
+    // meshes)
     std::vector<int> pslot;
     std::vector<double> pcoef;
     const bool node_form = s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML) &&
                            plan_node_pml(s, m, w, pslot, pcoef);
-    s->node_perm.clear();
-    s->node_inv.clear();
-    if (node_form) {
+    {
+        s->node_perm.clear();
+        s->node_inv.clear();
         s->node_perm.reserve(s->n_node);
-        for (int g = 0; g < s->n_node; ++g)
-            if (pslot[g] >= 0) s->node_perm.push_back(g);
-        for (int g = 0; g < s->n_node; ++g)
-            if (pslot[g] < 0) s->node_perm.push_back(g);
-        s->node_inv.assign(s->n_node, 0);
-        for (int d = 0; d < s->n_node; ++d) s->node_inv[s->node_perm[d]] = d;
+        std::vector<char> seen(s->n_node, 0);
+        for (int pass = node_form ? 0 : 1; pass < 2; ++pass)
+            for (long long q = 0; q < n_cell * nn; ++q) {
+                const int g = m->ibool[q];
+                if (seen[g] || (pass == 0 && pslot[g] < 0)) continue;
+                seen[g] = 1;
+                s->node_perm.push_back(g);
+            }
+        for (int g = 0; g < s->n_node; ++g)  // nodes no cell uses
+            if (!seen[g]) s->node_perm.push_back(g);
+        bool ident = true;
+        for (int d = 0; d < s->n_node && ident; ++d) ident = s->node_perm[d] == d;
+        if (ident) {
+            s->node_perm.clear();
+        } else {
+            s->node_inv.assign(s->n_node, 0);
+            for (int d = 0; d < s->n_node; ++d) s->node_inv[s->node_perm[d]] = d;
+        }
+        if (node_form) {
+            // slots follow the device order
+            const int n_slot = (int)(pcoef.size() / 14);
+            std::vector<double> c2(pcoef.size());
+            for (int d = 0; d < n_slot; ++d) {
+                const int g = s->node_perm.empty() ? d : s->node_perm[d];
+                std::copy(pcoef.begin() + (size_t)pslot[g] * 14, pcoef.begin() + (size_t)pslot[g] * 14 + 14,
+                          c2.begin() + (size_t)d * 14);
+            }
+            pcoef.swap(c2);
+        }
     }
     auto dev_node = [&](long long g) -> long long { return s->node_inv.empty() ? g : s->node_inv[g]; };
     auto permuted = [&](const std::vector<double>& h) {
@@ -968,6 +1010,34 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         s->n_pml = 0;
         for (long long e = 0; e < n_cell; ++e) s->n_pml += m->pml_region[e] != 0;
     }
+    // recording nodes: unique node ids in ascending order (the recording
+    // map's gll_node_ids), each node's (cell, point) occurrences, and the
+    // mass of each occurrence as the merge weight
+    if (s->n_rec > 0) {
+        std::vector<std::pair<int, int>> occ;  // (node, record index)
+        occ.reserve((size_t)s->n_rec * nn);
+        for (int ci = 0; ci < s->n_rec; ++ci)
+            for (int p = 0; p < nn; ++p)
+                occ.push_back({m->ibool[(size_t)m->rec_cell_local[ci] * nn + p], ci * nn + p});
+        std::sort(occ.begin(), occ.end());
+        std::vector<int> ptr{0}, idx;
+        std::vector<double> wts;
+        s->rec_node_ids.clear();
+        for (size_t k = 0; k < occ.size(); ++k) {
+            if (k == 0 || occ[k].first != occ[k - 1].first) {
+                if (k) ptr.push_back((int)k);
+                s->rec_node_ids.push_back(occ[k].first);
+            }
+            idx.push_back(occ[k].second);
+            const int ci = occ[k].second / nn, p = occ[k].second - ci * nn;
+            wts.push_back(m->mass[(size_t)m->rec_cell_local[ci] * nn + p]);
+        }
+        ptr.push_back((int)occ.size());
+        s->n_unique = (int)s->rec_node_ids.size();
+        if ((st = s->alloc(&s->gf_ptr, ptr.size())) || (st = h2d(s, s->gf_ptr, ptr.data(), ptr.size() * 4))) return st;
+        if ((st = s->alloc(&s->gf_occ, idx.size())) || (st = h2d(s, s->gf_occ, idx.data(), idx.size() * 4))) return st;
+        if ((st = s->alloc(&s->gf_w, wts.size())) || (st = h2d(s, s->gf_w, wts.data(), wts.size() * 8))) return st;
+    }
     // recording cells and snapshot ring
     if (s->n_rec > 0) {
         std::vector<int> rc(s->n_rec);
@@ -1119,6 +1189,19 @@ gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
         if (s->copy_issued[slot]) CU(cudaStreamWaitEvent(s->stream, s->copy_evt[slot], 0));
         void* dslot = static_cast<unsigned char*>(s->ring) + (size_t)slot * snapshot_bytes(s);
         if ((st = launch_record(s, dslot))) return st;
+        {
+            const long long total = (long long)s->nfld * s->n_unique * 15;
+            const int grid = grid_for(total, 256);
+            const long long per_field = (long long)s->n_rec * s->nn * 15;
+            if (s->rec_f32)
+                gfb::merge_nodes_kernel<float><<<grid, 256, 0, s->stream>>>(s->nfld, s->n_unique, per_field, s->gf_ptr,
+                                                                              s->gf_occ, s->gf_w, static_cast<float*>(dslot));
+            else
+                gfb::merge_nodes_kernel<double><<<grid, 256, 0, s->stream>>>(
+                    s->nfld, s->n_unique, per_field, s->gf_ptr, s->gf_occ, s->gf_w, static_cast<double*>(dslot));
+            CU(cudaGetLastError());
+            s->launches++;
+        }
         CU(cudaEventRecord(s->rec_evt[slot], s->stream));
         CU(cudaStreamWaitEvent(s->copy_stream, s->rec_evt[slot], 0));
         CU(cudaMemcpyAsync(s->pinned[slot], dslot, snapshot_bytes(s), cudaMemcpyDeviceToHost, s->copy_stream));
@@ -1685,6 +1768,63 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
             }
             if (release || snap->fields_read == s->nfld) snap->done = true;
         }
+        while (!s->pending.empty() && s->pending.front().done && s->pending.front().readers == 0)
+            s->pending.pop_front();
+    }
+    s->rec_cv.notify_all();
+    return st;
+}
+
+gfb_status gfb_rec_nodes(gfb_solver* s, int32_t* n_node, int64_t* node_ids) {
+    if (!s || !n_node) return fail(GFB_ERR_INVALID, "NULL argument");
+    *n_node = s->n_unique;
+    if (node_ids) std::memcpy(node_ids, s->rec_node_ids.data(), s->rec_node_ids.size() * 8);
+    return GFB_OK;
+}
+
+gfb_status gfb_read_green(gfb_solver* s, int32_t* step, double* strain, double* u, double* v, double* a,
+                          int32_t release) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    CU(cudaSetDevice(s->device));
+    Snapshot* snap;
+    int slot;
+    {
+        std::lock_guard<std::mutex> lk(s->rec_mu);
+        auto it = s->pending.begin();
+        while (it != s->pending.end() && it->done) ++it;
+        if (it == s->pending.end()) return fail(GFB_ERR_STATE, "no snapshot pending");
+        snap = &*it;
+        snap->readers++;
+        slot = snap->slot;
+    }
+    gfb_status st = GFB_OK;
+    if (slot >= 0 && cudaEventSynchronize(s->copy_evt[slot]) != cudaSuccess)
+        st = fail(GFB_ERR_CUDA, "snapshot copy failed");
+    const size_t nm = (size_t)s->nfld * s->n_unique * 15;
+    std::vector<double> buf(nm);
+    if (!st)
+        raw_values(s, slot >= 0 ? s->pinned[slot] : (const void*)snap->host.data(), snapshot_cell_values(s), nm,
+                   buf.data());
+    if (step) *step = snap->step;
+    if (!st) {
+        // [node][field][...]: the Green's tensor of a node is its fields' strains
+        for (int g = 0; g < s->n_unique; ++g)
+            for (int f = 0; f < s->nfld; ++f) {
+                const double* o = buf.data() + ((size_t)f * s->n_unique + g) * 15;
+                const size_t q = (size_t)g * s->nfld + f;
+                if (strain)
+                    for (int c = 0; c < 6; ++c) strain[q * 6 + c] = o[c];
+                for (int c = 0; c < 3; ++c) {
+                    if (u) u[q * 3 + c] = o[6 + c];
+                    if (v) v[q * 3 + c] = o[9 + c];
+                    if (a) a[q * 3 + c] = o[12 + c];
+                }
+            }
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->rec_mu);
+        snap->readers--;
+        if (!st && release) snap->done = true;
         while (!s->pending.empty() && s->pending.front().done && s->pending.front().readers == 0)
             s->pending.pop_front();
     }

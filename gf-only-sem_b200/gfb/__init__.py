@@ -138,6 +138,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.gfb_synchronize.argtypes = [C.c_void_p]
     lib.gfb_advance_profiled.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
     lib.gfb_advance_timed.argtypes = [C.c_void_p, C.c_int32, _dp]
+    lib.gfb_rec_nodes.argtypes = [C.c_void_p, _ip, _lp]
+    lib.gfb_read_green.argtypes = [C.c_void_p, _ip, _dp, _dp, _dp, _dp, C.c_int32]
     lib.gfb_checkpoint_size.argtypes = [C.c_void_p, _lp]
     lib.gfb_checkpoint_save.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     lib.gfb_checkpoint_load.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
@@ -157,6 +159,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "gfb_get_state", "gfb_set_state", "gfb_records_pending", "gfb_read_record",
         "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
         "gfb_create_batch", "gfb_checkpoint_size", "gfb_checkpoint_save", "gfb_checkpoint_load",
+        "gfb_rec_nodes", "gfb_read_green",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -338,6 +341,26 @@ class Solver:
         _check(self.lib.gfb_read_record(self.h, field, C.byref(step), _ptr(strain, C.c_double),
                                         _ptr(u, C.c_double), _ptr(v, C.c_double), _ptr(a, C.c_double),
                                         1 if release else 0))
+        return {"step": step.value, "strain": strain, "u": u, "v": v, "a": a}
+
+    def rec_nodes(self) -> np.ndarray:
+        """Node ids of the recording nodes (ascending)."""
+        n = C.c_int32()
+        _check(self.lib.gfb_rec_nodes(self.h, C.byref(n), _ptr(None, C.c_int64)))
+        ids = np.zeros(n.value, dtype=np.int64)
+        _check(self.lib.gfb_rec_nodes(self.h, C.byref(n), ids.ctypes.data_as(C.POINTER(C.c_int64))))
+        return ids
+
+    def read_green(self, release: bool = True):
+        """Oldest pending snapshot merged per recording node: strain
+        [node][field][6] (the Green's tensor with fields x, y, z), u, v, a
+        [node][field][3]."""
+        n = len(self.rec_nodes())
+        step = C.c_int32()
+        strain = np.zeros((n, self.n_field, 6))
+        u, v, a = (np.zeros((n, self.n_field, 3)) for _ in range(3))
+        _check(self.lib.gfb_read_green(self.h, C.byref(step), _ptr(strain, C.c_double), _ptr(u, C.c_double),
+                                       _ptr(v, C.c_double), _ptr(a, C.c_double), 1 if release else 0))
         return {"step": step.value, "strain": strain, "u": u, "v": v, "a": a}
 
     def drain(self):

@@ -325,11 +325,20 @@ def surface_records(prob: dict, snaps: dict, shift: float):
     return key, np.asarray(snaps["u"])  # [n_snap][n_rec][nn][3]
 
 
-def reflection_error(thin: dict, thin_snaps: dict, thick: dict, thick_snaps: dict, shift: float) -> float:
+def surface_keys(prob: dict, shift: float = 0.0) -> np.ndarray:
+    """Cell-centre keys of the recorded cells (see surface_records)."""
+    return surface_records(prob, {"u": np.zeros(0)}, shift)[0]
+
+
+def reflection_error(thin: dict, thin_snaps: dict, thick, thick_snaps: dict, shift: float) -> float:
     """||u_thin - u_thick|| / ||u_thick|| over every snapshot of the thin
-    domain's recorded interior surface cells."""
+    domain's recorded interior surface cells; `thick` is the thick problem
+    or its surface_keys."""
     ka, ua = surface_records(thin, thin_snaps, shift)
-    kb, ub = surface_records(thick, thick_snaps, 0.0)
+    if isinstance(thick, dict):
+        kb, ub = surface_records(thick, thick_snaps, 0.0)
+    else:
+        kb, ub = thick, np.asarray(thick_snaps["u"])
     idx = {tuple(k): i for i, k in enumerate(kb)}
     sel = [i for i, k in enumerate(ka) if tuple(k) in idx]
     if not sel:

@@ -249,6 +249,24 @@ gfb_status gfb_set_state(gfb_solver* solver, int32_t field, int32_t step, const 
                          const double* v, const double* a);
 
 /*
+ * Strain Green's functions at the recording nodes.  Recording cells share
+ * GLL nodes; each snapshot also holds its values merged per node, as the
+ * reference's post-processing does (postprocess/cpp/main.cpp:300-425):
+ * strain weighted by the lumped mass of each (cell, point) occurrence
+ * (sum m e / sum m), u, v, a averaged over the occurrences.  The reference
+ * divides its accumulated displacement by the mass sum too (main.cpp:419-423,
+ * a unit mismatch unless the masses are 1); here displacement is the plain
+ * average.  gfb_rec_nodes gives the node count and ids (ascending: the
+ * recording map's gll_node_ids); gfb_read_green reads the oldest pending
+ * snapshot for every wavefield at once: strain [node][field][6] (with
+ * field_dir = {x, y, z} this is the 3 x 6 Green's tensor of main.cpp:540-560
+ * per node), u, v, a [node][field][3]; release != 0 consumes the snapshot.
+ */
+gfb_status gfb_rec_nodes(gfb_solver* solver, int32_t* n_node, int64_t* node_ids);
+gfb_status gfb_read_green(gfb_solver* solver, int32_t* step, double* strain, double* u, double* v, double* a,
+                          int32_t release);
+
+/*
  * Exact checkpoint of the time loop: u, v, a, the predicted displacement,
  * the C-PML memory and previous fields (per cell or per node) and the step
  * counters, in the device layout.  The reference's restart file keeps u, v,
