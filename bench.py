@@ -82,7 +82,9 @@ METRIC = "GLL-point updates/s (FP32 batched x/y/z, 1 B200)"
 UNIT = "GLL-pt/s"
 
 
-def build_workload(name: str):
+def build_workload(name: str, device=None):
+    """Inputs of a named workload; ``device`` = a GPU index computes the
+    geometry, numbering and C-PML coefficients there (gfb.prep)."""
     from gfb import mesh
 
     w = WORKLOADS[name]
@@ -104,7 +106,7 @@ def build_workload(name: str):
     else:
         mat = mesh.homogeneous()
     return mesh.build_problem(spec, mat, np.array(w["src"]), nsteps=w["nsteps"], snapshot_stride=w["stride"],
-                              record_depth_max_m=w["depth"], record_tile=tile)
+                              record_depth_max_m=w["depth"], record_tile=tile, device=device)
 
 
 def batch_specs(seed: int = BATCH["seed"], n_model: int = BATCH["n_model"]):
@@ -639,13 +641,13 @@ def run_gfb(args):
     s.close()
 
     # end to end through the public API from host arrays: create (upload and
-    # set-up), K steps, every snapshot read back to host, destroy
+    # set-up), K steps with every snapshot read into host arrays by a second
+    # thread as it arrives (Solver.run), destroy
     t0 = time.perf_counter()
     s2 = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8, flags=flags)
     t_create = time.perf_counter() - t0
     up = s2.info()["upload_bytes"]
-    s2.advance(args.steps)
-    rec = s2.drain()
+    rec = s2.run(args.steps)
     s2.synchronize()
     s2.close()
     e2e_t = time.perf_counter() - t0
@@ -684,7 +686,8 @@ def run_gfb(args):
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": up / args.steps,
                 "d2h_bytes_per_step": rec_bytes / args.steps,
                 "create_s": t_create, "total_s": e2e_t,
-                "note": "gfb_create from host arrays + K steps + all snapshots read to host + destroy"},
+                "note": "gfb_create from host arrays + K steps with every snapshot read into host arrays "
+                        "(Solver.run) + destroy"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

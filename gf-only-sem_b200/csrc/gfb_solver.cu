@@ -5,9 +5,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -96,10 +98,12 @@ bool gll_tables(int N, std::vector<double>& x, std::vector<double>& w, std::vect
     return true;
 }
 
+// fn(i0, i1) over [0, n) split across the host's threads, each thread
+// taking at least `grain` items
 template <typename F>
-void parallel_for(long long n, F&& fn) {
+void parallel_for(long long n, F&& fn, long long grain = 65536) {
     unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    if (n < 65536) nt = 1;
+    nt = (unsigned)std::max(1LL, std::min((long long)nt, n / std::max(1LL, grain)));
     if (nt == 1) {
         fn(0LL, n);
         return;
@@ -119,7 +123,7 @@ struct DevBuf {
 struct Snapshot {
     int step;
     int slot;                  // ring slot (device + pinned host), -1 once spilled
-    std::vector<unsigned char> host;  // spilled raw copy [NFLD][n_rec][NN][15] (float or double)
+    std::unique_ptr<unsigned char[]> host;  // spilled raw copy [NFLD][n_rec][NN][15] (float or double)
     int fields_read = 0;
     int readers = 0;           // gfb_read_record calls copying out of the slot
     bool done = false;         // read (or released); removed once no reader holds it
@@ -262,6 +266,66 @@ gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
     *dst = d;
     return GFB_OK;
 }
+
+// Pinned staging buffers of staged_upload; the destructor waits for the
+// copies still reading them.
+struct Staging {
+    void* buf[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    ~Staging() {
+        for (int k = 0; k < 2; ++k) {
+            if (done[k]) {
+                cudaEventSynchronize(done[k]);
+                cudaEventDestroy(done[k]);
+            }
+            if (buf[k]) cudaFreeHost(buf[k]);
+        }
+    }
+};
+
+// Fill the device array dst of n_item items of item_bytes each.  The host
+// threads pack the items chunk by chunk (pack(i0, i1, out) writes items
+// [i0, i1) to out) into two pinned staging buffers in turn, and the copy of
+// one chunk to the device runs while the next is packed: no host copy of the
+// whole array and no copy from pageable memory.
+template <typename Pack>
+gfb_status staged_upload(gfb_solver* s, void* dst, size_t item_bytes, long long n_item, Pack&& pack) {
+    if (n_item <= 0) return GFB_OK;
+    const size_t stage = size_t(64) << 20;
+    const long long per = std::max<long long>(1, (long long)(stage / item_bytes));
+    const size_t bytes = (size_t)std::min<long long>(per, n_item) * item_bytes;
+    Staging S;
+    for (int k = 0; k < 2; ++k) {
+        CU(cudaHostAlloc(&S.buf[k], bytes, cudaHostAllocDefault));
+        CU(cudaEventCreateWithFlags(&S.done[k], cudaEventDisableTiming));
+    }
+    long long c = 0;
+    for (long long i0 = 0; i0 < n_item; i0 += per, ++c) {
+        const int k = (int)(c & 1);
+        const long long i1 = std::min(n_item, i0 + per);
+        CU(cudaEventSynchronize(S.done[k]));  // the copy of chunk c-2 has read the buffer
+        pack(i0, i1, static_cast<unsigned char*>(S.buf[k]));
+        CU(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + (size_t)i0 * item_bytes, S.buf[k],
+                           (size_t)(i1 - i0) * item_bytes, cudaMemcpyHostToDevice, s->stream));
+        CU(cudaEventRecord(S.done[k], s->stream));
+    }
+    CU(cudaStreamSynchronize(s->stream));
+    s->upload_bytes += (long long)((size_t)n_item * item_bytes);
+    return GFB_OK;
+}
+
+// Seconds spent in each stage of gfb_create, printed to stderr when the
+// environment variable GFB_TRACE is set.
+struct StageClock {
+    bool on = std::getenv("GFB_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char* what) {
+        if (!on) return;
+        const auto n = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "gfb_create %-28s %8.3f s\n", what, std::chrono::duration<double>(n - t).count());
+        t = n;
+    }
+};
 
 // ---------------------------------------------------------------------------
 // kernel dispatch
@@ -636,13 +700,29 @@ size_t snapshot_bytes(const gfb_solver* s) { return snapshot_values(s) * (s->rec
 
 // Convert n snapshot values starting at value `off` of a raw snapshot
 // (float or double, as recorded) to double.
-void raw_values(const gfb_solver* s, const void* raw, size_t off, size_t n, double* dst) {
-    if (s->rec_f32) {
-        const float* src = static_cast<const float*>(raw) + off;
-        for (size_t i = 0; i < n; ++i) dst[i] = src[i];
-    } else {
-        std::memcpy(dst, static_cast<const double*>(raw) + off, n * sizeof(double));
-    }
+// Scatter n_out recorded points of 15 values (strain 6, u 3, v 3, a 3) into
+// the caller's arrays: output point q takes the 15 values at
+// raw + src_index(q) * 15 (float or double as recorded).  Threads split the
+// points; a NULL array is skipped.
+template <typename Index>
+void unpack_points(const gfb_solver* s, const void* raw, long long n_out, Index src_index, double* strain, double* u,
+                   double* v, double* a) {
+    auto run = [&](auto* src) {
+        parallel_for(n_out, [&](long long q0, long long q1) {
+            for (long long q = q0; q < q1; ++q) {
+                const auto* o = src + (size_t)src_index(q) * 15;
+                if (strain)
+                    for (int c = 0; c < 6; ++c) strain[q * 6 + c] = (double)o[c];
+                for (int c = 0; c < 3; ++c) {
+                    if (u) u[q * 3 + c] = (double)o[6 + c];
+                    if (v) v[q * 3 + c] = (double)o[9 + c];
+                    if (a) a[q * 3 + c] = (double)o[12 + c];
+                }
+            }
+        }, 16384);
+    };
+    if (s->rec_f32) run(static_cast<const float*>(raw));
+    else run(static_cast<const double*>(raw));
 }
 
 // Copy a snapshot out of its pinned slot into pageable memory, as recorded,
@@ -650,8 +730,15 @@ void raw_values(const gfb_solver* s, const void* raw, size_t off, size_t n, doub
 // yet).
 gfb_status spill(gfb_solver* s, Snapshot& snap) {
     CU(cudaEventSynchronize(s->copy_evt[snap.slot]));
-    snap.host.resize(snapshot_bytes(s));
-    std::memcpy(snap.host.data(), s->pinned[snap.slot], snap.host.size());
+    const size_t n = snapshot_bytes(s);
+    snap.host.reset(new unsigned char[n]);  // no zero fill: every byte is copied below
+    unsigned char* dst = snap.host.get();
+    const unsigned char* src = static_cast<const unsigned char*>(s->pinned[snap.slot]);
+    const size_t chunk = 1 << 16;
+    parallel_for((long long)((n + chunk - 1) / chunk), [&](long long c0, long long c1) {
+        const size_t b0 = (size_t)c0 * chunk, b1 = std::min(n, (size_t)c1 * chunk);
+        std::memcpy(dst + b0, src + b0, b1 - b0);
+    }, 32);
     snap.slot = -1;
     return GFB_OK;
 }
@@ -746,7 +833,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
                         const gfb_model* models, const std::vector<int>& perm, const std::vector<int>& inv_perm,
                         const std::vector<uint32_t>& ibool_dev, const std::vector<double>& node_mass,
                         const std::vector<double>& node_damp, const std::vector<double>& w,
-                        const std::vector<double>& D) {
+                        const std::vector<double>& D, StageClock& clk) {
     const int ng = s->ng, nn = s->nn;
     const long long n_cell = s->n_cell;
     gfb_status st;
@@ -795,6 +882,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
             pcoef.swap(c2);
         }
     }
+    clk.mark("node numbering");
     auto dev_node = [&](long long g) -> long long { return s->node_inv.empty() ? g : s->node_inv[g]; };
     auto permuted = [&](const std::vector<double>& h) {
         if (s->node_perm.empty()) return h;
@@ -802,51 +890,70 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         for (size_t d = 0; d < o.size(); ++d) o[d] = h[s->node_perm[d]];
         return o;
     };
-    // ibool
+    // ibool in device node numbers, and the rows of the pipelined kernels:
+    // node words, then the cell's model, zero padding
     {
-        std::vector<uint32_t> ibd(ibool_dev);
-        if (!s->node_inv.empty())
-            for (auto& x : ibd) x = (x & ~gfb::kNodeMask) | (uint32_t)s->node_inv[x & gfb::kNodeMask];
+        auto dev_word = [&](uint32_t x) {
+            return s->node_inv.empty() ? x
+                                       : (x & ~gfb::kNodeMask) | (uint32_t)s->node_inv[x & gfb::kNodeMask];
+        };
         uint32_t* d = nullptr;
-        if ((st = s->alloc(&d, ibd.size()))) return st;
-        if ((st = h2d(s, d, ibd.data(), ibd.size() * 4))) return st;
+        if ((st = s->alloc(&d, (size_t)n_cell * nn))) return st;
+        st = staged_upload(s, d, (size_t)nn * 4, n_cell, [&](long long e0, long long e1, unsigned char* out) {
+            uint32_t* o = reinterpret_cast<uint32_t*>(out);
+            parallel_for(e1 - e0, [&](long long a0, long long a1) {
+                for (long long i = a0 * nn; i < a1 * nn; ++i) o[i] = dev_word(ibool_dev[e0 * nn + i]);
+            }, 1024);
+        });
+        if (st) return st;
         s->ibool = d;
-        // rows of the pipelined kernels: node words, then the cell's model
         const int nnp = gfb::ib_row_words(nn);
-        std::vector<uint32_t> pad((size_t)n_cell * nnp, 0u);
-        int mi = 0;
-        for (long long e = 0; e < n_cell; ++e) {
-            for (int p = 0; p < nn; ++p) pad[e * nnp + p] = ibd[e * nn + p];
-            const int orig = perm[e];
-            mi = 0;
-            while (orig >= models[mi].cell_end) ++mi;
-            pad[e * nnp + nn] = (uint32_t)mi;
-        }
         uint32_t* dp = nullptr;
-        if ((st = s->alloc(&dp, pad.size()))) return st;
-        if ((st = h2d(s, dp, pad.data(), pad.size() * 4))) return st;
+        if ((st = s->alloc(&dp, (size_t)n_cell * nnp))) return st;
+        st = staged_upload(s, dp, (size_t)nnp * 4, n_cell, [&](long long e0, long long e1, unsigned char* out) {
+            uint32_t* o = reinterpret_cast<uint32_t*>(out);
+            parallel_for(e1 - e0, [&](long long a0, long long a1) {
+                for (long long i = a0; i < a1; ++i) {
+                    const long long e = e0 + i;
+                    uint32_t* row = o + i * nnp;
+                    for (int p = 0; p < nn; ++p) row[p] = dev_word(ibool_dev[e * nn + p]);
+                    int mi = 0;
+                    while (perm[e] >= models[mi].cell_end) ++mi;
+                    row[nn] = (uint32_t)mi;
+                    for (int p = nn + 1; p < nnp; ++p) row[p] = 0u;
+                }
+            }, 1024);
+        });
+        if (st) return st;
         s->ibool_padded = dp;
     }
+    clk.mark("ibool upload");
     // geometry [cell][12][NN] in colour order
     {
-        std::vector<Real> g((size_t)n_cell * 12 * nn);
-        parallel_for(n_cell, [&](long long e0, long long e1) {
-            for (long long ed = e0; ed < e1; ++ed) {
-                const long long e = perm[ed];
-                Real* o = g.data() + ed * 12 * nn;
-                for (int p = 0; p < nn; ++p) {
-                    const long long q = e * nn + p;
-                    for (int f = 0; f < 9; ++f) o[f * nn + p] = (Real)m->dxi_dx[q * 9 + f];
-                    const int i = p / (ng * ng), j = (p / ng) % ng, k = p % ng;
-                    // factor = detJ * w_i * w_j * w_k (element_cpu.cpp:108)
-                    o[9 * nn + p] = (Real)(m->jacobian[q] * w[i] * w[j] * w[k]);
-                    o[10 * nn + p] = (Real)m->lambda_[q];
-                    o[11 * nn + p] = (Real)m->mu[q];
+        Real* dg = nullptr;
+        if ((st = s->alloc(&dg, (size_t)n_cell * 12 * nn))) return st;
+        st = staged_upload(s, dg, (size_t)12 * nn * sizeof(Real), n_cell,
+                           [&](long long e0, long long e1, unsigned char* out) {
+            parallel_for(e1 - e0, [&](long long a0, long long a1) {
+                for (long long i = a0; i < a1; ++i) {
+                    const long long e = perm[e0 + i];
+                    Real* o = reinterpret_cast<Real*>(out) + i * 12 * nn;
+                    for (int p = 0; p < nn; ++p) {
+                        const long long q = e * nn + p;
+                        for (int f = 0; f < 9; ++f) o[f * nn + p] = (Real)m->dxi_dx[q * 9 + f];
+                        const int i0 = p / (ng * ng), j = (p / ng) % ng, k = p % ng;
+                        // factor = detJ * w_i * w_j * w_k (element_cpu.cpp:108)
+                        o[9 * nn + p] = (Real)(m->jacobian[q] * w[i0] * w[j] * w[k]);
+                        o[10 * nn + p] = (Real)m->lambda_[q];
+                        o[11 * nn + p] = (Real)m->mu[q];
+                    }
                 }
-            }
+            }, 256);
         });
-        if ((st = upload(s, &s->geom, g))) return st;
+        if (st) return st;
+        s->geom = dg;
     }
+    clk.mark("geometry upload");
     {
         std::vector<Real> d(D.size());
         for (size_t i = 0; i < D.size(); ++i) d[i] = (Real)D[i];
@@ -907,11 +1014,14 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
             if ((st = h2d(s, d, slot.data(), slot.size() * 4))) return st;
             s->pml_slot = d;
         }
-        std::vector<Real> coef((size_t)s->n_pml * 15 * nn);
-        parallel_for(s->n_pml, [&](long long a0, long long a1) {
-            for (long long sl = a0; sl < a1; ++sl) {
-                const long long e = slot_cell[sl];
-                Real* o = coef.data() + sl * 15 * nn;
+        Real* dcoef = nullptr;
+        if ((st = s->alloc(&dcoef, (size_t)s->n_pml * 15 * nn))) return st;
+        st = staged_upload(s, dcoef, (size_t)15 * nn * sizeof(Real), s->n_pml,
+                           [&](long long s0, long long s1, unsigned char* out) {
+          parallel_for(s1 - s0, [&](long long a0, long long a1) {
+            for (long long i = a0; i < a1; ++i) {
+                const long long e = slot_cell[s0 + i];
+                Real* o = reinterpret_cast<Real*>(out) + i * 15 * nn;
                 for (int p = 0; p < nn; ++p) {
                     const long long q = e * nn + p;
                     for (int f = 0; f < 9; ++f) o[f * nn + p] = (Real)m->pml_coef_alpha[q * 9 + f];
@@ -923,8 +1033,10 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
                     o[14 * nn + p] = (Real)(wgll * rho_inv * m->jacobian[q]);
                 }
             }
+          }, 256);
         });
-        if ((st = upload(s, &s->pml_coef, coef))) return st;
+        if (st) return st;
+        s->pml_coef = dcoef;
         Real *mem = nullptr, *prev = nullptr;
         if ((st = s->alloc(&mem, (size_t)s->n_pml * s->F * 3 * nn))) return st;
         if ((st = s->alloc(&prev, (size_t)s->n_pml * s->F * nn))) return st;
@@ -1270,27 +1382,60 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
 
+    StageClock clk;
     const int nn = s->nn;
     const long long P = (long long)m->n_cell * nn;
     // ibool range and per-cell distinctness (a repeated node inside one cell
-    // would make two threads of one block update the same force entry)
-    std::vector<int> mark(m->n_node, -1);
-    for (long long e = 0; e < m->n_cell; ++e)
-        for (int p = 0; p < nn; ++p) {
-            const int g = m->ibool[e * nn + p];
-            if (g < 0 || g >= m->n_node)
-                return fail(GFB_ERR_INVALID, "ibool[%lld]=%d outside [0,%d)", e * nn + p, g, m->n_node);
-            if (mark[g] == (int)e)
-                return fail(GFB_ERR_INVALID, "cell %lld lists node %d twice", e, g);
-            mark[g] = (int)e;
+    // would make two threads of one block update the same force entry); the
+    // first offending entry in mesh order is reported: an entry out of range,
+    // or the second occurrence of a node in its cell
+    {
+        std::mutex bad_mu;
+        long long bad_q = -1;
+        bool bad_range = false;
+        parallel_for(m->n_cell, [&](long long e0, long long e1) {
+            std::vector<uint64_t> key(nn);
+            for (long long e = e0; e < e1; ++e) {
+                int rng_at = nn, dup_at = nn;
+                for (int p = 0; p < nn; ++p) {
+                    const int g = m->ibool[e * nn + p];
+                    if (rng_at == nn && (g < 0 || g >= m->n_node)) rng_at = p;
+                    key[p] = ((uint64_t)(uint32_t)g << 32) | (uint32_t)p;
+                }
+                std::sort(key.begin(), key.end());
+                for (int k = 1; k < nn; ++k)
+                    if ((key[k] >> 32) == (key[k - 1] >> 32)) dup_at = std::min(dup_at, (int)(key[k] & 0xffffffffu));
+                const int at = std::min(rng_at, dup_at);
+                if (at < nn) {
+                    std::lock_guard<std::mutex> lk(bad_mu);
+                    if (bad_q < 0 || e * nn + at < bad_q) {
+                        bad_q = e * nn + at;
+                        bad_range = at == rng_at;
+                    }
+                    return;  // later cells of this range come after it
+                }
+            }
+        }, 4096);
+        if (bad_q >= 0) {
+            if (bad_range)
+                return fail(GFB_ERR_INVALID, "ibool[%lld]=%d outside [0,%d)", bad_q, m->ibool[bad_q], m->n_node);
+            return fail(GFB_ERR_INVALID, "cell %lld lists node %d twice", bad_q / nn, m->ibool[bad_q]);
         }
-    // global lumped mass (accumulate) and damping (assign), solver.cpp:193-202
-    std::vector<double> node_mass(m->n_node, 0.0), node_damp(m->n_node, 0.0);
-    for (long long q = 0; q < P; ++q) {
-        const int g = m->ibool[q];
-        node_mass[g] += m->mass[q];
-        node_damp[g] = m->damping ? m->damping[q] : 0.0;
     }
+    clk.mark("mesh check");
+    // global lumped mass (accumulate) and damping (assign), solver.cpp:193-202.
+    // Each thread owns a range of nodes and scans every entry in mesh order,
+    // so every node sums (and assigns) in the reference's order
+    std::vector<double> node_mass(m->n_node, 0.0), node_damp(m->n_node, 0.0);
+    parallel_for(m->n_node, [&](long long g0, long long g1) {
+        for (long long q = 0; q < P; ++q) {
+            const int g = m->ibool[q];
+            if (g < g0 || g >= g1) continue;
+            node_mass[g] += m->mass[q];
+            node_damp[g] = m->damping ? m->damping[q] : 0.0;
+        }
+    }, 1 << 18);
+    clk.mark("lumped mass");
     s->has_damping = false;
     if (!s->has_cpml && m->damping)
         for (double d : node_damp)
@@ -1312,6 +1457,7 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
         n_colour = std::max(n_colour, col + 1);
         for (int p = 0; p < nn; ++p) used[m->ibool[e * nn + p]] |= (1ull << col);
     }
+    clk.mark("colouring");
     std::vector<int> perm(m->n_cell), inv_perm(m->n_cell);
     s->colour_begin.assign(n_colour + 1, 0);
     for (long long e = 0; e < m->n_cell; ++e) s->colour_begin[colour[e] + 1]++;
@@ -1339,21 +1485,24 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
             }
         }
     });
+    clk.mark("colour order");
     std::vector<double> x, w, D;
     if (!gll_tables(m->ngll - 1, x, w, D)) return fail(GFB_ERR_INVALID, "GLL table construction failed");
     if (s->prec == GFB_FP64) {
         if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<double>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                  w, D);
+                                  w, D, clk);
     } else {
         if ((st = dispatch<float, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<float>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                 w, D);
+                                 w, D, clk);
     }
     if (st) return st;
     CU(cudaStreamSynchronize(s->stream));
+    clk.mark("device set-up");
     if ((c->flags & GFB_FLAG_AUTOTUNE) && (st = autotune(s.get()))) return st;
     CU(cudaDeviceSynchronize());
+    clk.mark("autotune");
     *out = s.release();
     return GFB_OK;
 }
@@ -1719,7 +1868,6 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
     CU(cudaSetDevice(s->device));
-    const size_t per_field = (size_t)s->n_rec * s->nn * 15;
     Snapshot* snap;
     int slot;
     {
@@ -1732,31 +1880,15 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
         slot = snap->slot;
     }
     // copy out without holding the lock (the stepping thread may go on)
-    std::vector<double> buf;
-    const double* src = nullptr;
-    const bool want = strain || u || v || a;
     gfb_status st = GFB_OK;
     if (slot >= 0 && cudaEventSynchronize(s->copy_evt[slot]) != cudaSuccess)
         st = fail(GFB_ERR_CUDA, "snapshot copy failed");
-    if (want) {
-        buf.resize(per_field);
-        if (!st) raw_values(s, slot >= 0 ? s->pinned[slot] : (const void*)snap->host.data(), field * per_field,
-                            per_field, buf.data());
-        src = buf.data();
-    }
     if (step) *step = snap->step;
-    if (!st && want) {
-        const size_t npt = (size_t)s->n_rec * s->nn;
-        for (size_t q = 0; q < npt; ++q) {
-            const double* o = src + q * 15;
-            if (strain)
-                for (int c = 0; c < 6; ++c) strain[q * 6 + c] = o[c];
-            for (int c = 0; c < 3; ++c) {
-                if (u) u[q * 3 + c] = o[6 + c];
-                if (v) v[q * 3 + c] = o[9 + c];
-                if (a) a[q * 3 + c] = o[12 + c];
-            }
-        }
+    if (!st && (strain || u || v || a)) {
+        const void* raw = slot >= 0 ? s->pinned[slot] : (const void*)snap->host.get();
+        const long long first = (long long)field * s->n_rec * s->nn;  // points of the earlier fields
+        unpack_points(s, raw, (long long)s->n_rec * s->nn, [first](long long q) { return first + q; }, strain, u,
+                      v, a);
     }
     {
         std::lock_guard<std::mutex> lk(s->rec_mu);
@@ -1800,26 +1932,16 @@ gfb_status gfb_read_green(gfb_solver* s, int32_t* step, double* strain, double* 
     gfb_status st = GFB_OK;
     if (slot >= 0 && cudaEventSynchronize(s->copy_evt[slot]) != cudaSuccess)
         st = fail(GFB_ERR_CUDA, "snapshot copy failed");
-    const size_t nm = (size_t)s->nfld * s->n_unique * 15;
-    std::vector<double> buf(nm);
-    if (!st)
-        raw_values(s, slot >= 0 ? s->pinned[slot] : (const void*)snap->host.data(), snapshot_cell_values(s), nm,
-                   buf.data());
     if (step) *step = snap->step;
     if (!st) {
+        // merged part [field][node][15] after the cell part, read out as
         // [node][field][...]: the Green's tensor of a node is its fields' strains
-        for (int g = 0; g < s->n_unique; ++g)
-            for (int f = 0; f < s->nfld; ++f) {
-                const double* o = buf.data() + ((size_t)f * s->n_unique + g) * 15;
-                const size_t q = (size_t)g * s->nfld + f;
-                if (strain)
-                    for (int c = 0; c < 6; ++c) strain[q * 6 + c] = o[c];
-                for (int c = 0; c < 3; ++c) {
-                    if (u) u[q * 3 + c] = o[6 + c];
-                    if (v) v[q * 3 + c] = o[9 + c];
-                    if (a) a[q * 3 + c] = o[12 + c];
-                }
-            }
+        const void* raw = slot >= 0 ? s->pinned[slot] : (const void*)snap->host.get();
+        const long long cells = (long long)(snapshot_cell_values(s) / 15);
+        const int nfld = s->nfld;
+        const long long nu = s->n_unique;
+        unpack_points(s, raw, nu * nfld,
+                      [=](long long q) { return cells + (q % nfld) * nu + q / nfld; }, strain, u, v, a);
     }
     {
         std::lock_guard<std::mutex> lk(s->rec_mu);

@@ -241,6 +241,7 @@ class Solver:
         c = Config()
         c.dt = float(prob["dt"])
         c.snapshot_stride = int(prob.get("snapshot_stride", 0))
+        self.stride = c.snapshot_stride
         c.precision = int(precision)
         c.n_field = len(dirs)
         for i, d in enumerate(dirs):
@@ -334,14 +335,32 @@ class Solver:
         _check(self.lib.gfb_records_pending(self.h, C.byref(n)))
         return n.value
 
-    def read_record(self, field: int = 0, release: bool = False):
+    def _record_arrays(self, n: Optional[int] = None):
+        lead = () if n is None else (n,)
+        out = {"strain": np.empty(lead + (self.n_rec, self.nn, 6))}
+        for k in ("u", "v", "a"):
+            out[k] = np.empty(lead + (self.n_rec, self.nn, 3))
+        return out
+
+    def read_record(self, field: int = 0, release: bool = False, out: Optional[dict] = None):
+        """Oldest unread snapshot of one field: strain [cell][point][6],
+        u, v, a [cell][point][3] over the recording cells.  ``out`` gives
+        C-contiguous float64 arrays of those shapes to fill instead of new
+        ones (a missing key is not read)."""
         step = C.c_int32()
-        strain = np.zeros((self.n_rec, self.nn, 6))
-        u, v, a = (np.zeros((self.n_rec, self.nn, 3)) for _ in range(3))
-        _check(self.lib.gfb_read_record(self.h, field, C.byref(step), _ptr(strain, C.c_double),
-                                        _ptr(u, C.c_double), _ptr(v, C.c_double), _ptr(a, C.c_double),
+        if out is None:
+            out = self._record_arrays()
+        arrs = {}
+        for k, last in (("strain", 6), ("u", 3), ("v", 3), ("a", 3)):
+            x = out.get(k)
+            if x is not None and (x.dtype != np.float64 or not x.flags.c_contiguous
+                                  or x.shape != (self.n_rec, self.nn, last)):
+                raise ValueError(f"out[{k!r}] must be C-contiguous float64 of shape {(self.n_rec, self.nn, last)}")
+            arrs[k] = x
+        _check(self.lib.gfb_read_record(self.h, field, C.byref(step),
+                                        *[_ptr(arrs[k], C.c_double) for k in ("strain", "u", "v", "a")],
                                         1 if release else 0))
-        return {"step": step.value, "strain": strain, "u": u, "v": v, "a": a}
+        return {"step": step.value, **arrs}
 
     def rec_nodes(self) -> np.ndarray:
         """Node ids of the recording nodes (ascending)."""
@@ -363,19 +382,63 @@ class Solver:
                                        _ptr(v, C.c_double), _ptr(a, C.c_double), 1 if release else 0))
         return {"step": step.value, "strain": strain, "u": u, "v": v, "a": a}
 
+    def _read_snapshots(self, n: int, wait=None):
+        """n snapshots, every field, read into arrays allocated once:
+        {field: {"steps": [n], "strain": [n][cell][point][6], "u"/"v"/"a":
+        [n][cell][point][3]}}.  ``wait()`` is called while none is pending
+        (returns False to give up)."""
+        out = {}
+        for f in range(self.n_field):
+            out[f] = {"steps": np.zeros(n, dtype=np.int64), **self._record_arrays(n)}
+        for i in range(n):
+            while wait is not None and self.pending() == 0:
+                if not wait():
+                    raise GfbError(3, "snapshot reader stopped before all snapshots arrived")
+            for f in range(self.n_field):
+                r = self.read_record(f, out={k: out[f][k][i] for k in ("strain", "u", "v", "a")})
+                out[f]["steps"][i] = r["step"]
+        return out
+
     def drain(self):
         """All pending snapshots as {field: dict of stacked arrays}."""
-        out = {f: {"steps": [], "strain": [], "u": [], "v": [], "a": []} for f in range(self.n_field)}
-        while self.pending() > 0:
-            for f in range(self.n_field):
-                r = self.read_record(f)
-                out[f]["steps"].append(r["step"])
-                for k in ("strain", "u", "v", "a"):
-                    out[f][k].append(r[k])
-        for f in out:
-            for k in out[f]:
-                out[f][k] = np.array(out[f][k])
-        return out
+        return self._read_snapshots(self.pending())
+
+    def run(self, n_steps: int):
+        """Advance n_steps and return every snapshot pending before them or
+        recorded by them (as ``drain``), read out by a second thread while the
+        steps run, as the reference's time loop writes each snapshot when it
+        is taken."""
+        import threading
+
+        first = self.step
+        n = self.pending()
+        if self.stride > 0 and self.n_rec > 0:
+            n += sum(1 for t in range(first, first + int(n_steps)) if t % self.stride == 0)
+        done = threading.Event()
+        box = {}
+
+        def wait():
+            if done.is_set() and self.pending() == 0:
+                return False
+            done.wait(0.0002)
+            return True
+
+        def reader():
+            try:
+                box["out"] = self._read_snapshots(n, wait)
+            except BaseException as e:  # re-raised in the caller's thread
+                box["err"] = e
+
+        th = threading.Thread(target=reader, daemon=True)
+        th.start()
+        try:
+            self.advance(n_steps)
+        finally:
+            done.set()
+            th.join()
+        if "err" in box:
+            raise box["err"]
+        return box["out"]
 
     def close(self):
         if getattr(self, "h", None):

@@ -729,11 +729,20 @@ def build_problem(
     amp: float = 1.0e20,
     with_cpml: bool = True,
     record_tile=None,
+    device: Optional[int] = None,
 ) -> dict:
-    """Every solver input for one synthetic model, reference layouts."""
+    """Every solver input for one synthetic model, reference layouts.
+
+    ``device`` = a GPU index computes the GLL geometry, the node numbering
+    and the C-PML coefficients there (``gfb.prep``) instead of on the host."""
+    if device is not None:
+        from . import prep
     V = vertex_grid(spec)
     corners = cell_corners(spec, V)
-    coords, jac, dxi, mgeo = gll_geometry(corners, spec.order)
+    if device is None:
+        coords, jac, dxi, mgeo = gll_geometry(corners, spec.order)
+    else:
+        coords, jac, dxi, mgeo = prep.gll_geometry(corners, spec.order, device=device)
     bounds = {
         "xmin": float(V[..., 0].min()),
         "xmax": float(V[..., 0].max()),
@@ -749,7 +758,7 @@ def build_problem(
     if dt is None:
         dt = cfl * h_min(coords) / float(vp.max())
     is_pml = pml_flags(spec)
-    ibool, n_node = global_numbering(coords)
+    ibool, n_node = global_numbering(coords) if device is None else prep.global_numbering(coords, device=device)
     widths = {
         "xmin": spec.pml.get("xmin", 0) * (bounds["xmax"] - bounds["xmin"]) / spec.nx,
         "xmax": spec.pml.get("xmax", 0) * (bounds["xmax"] - bounds["xmin"]) / spec.nx,
@@ -781,7 +790,10 @@ def build_problem(
         "snapshot_stride": int(snapshot_stride),
     }
     if with_cpml:
-        region, calpha, abar = cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt)
+        if device is None:
+            region, calpha, abar = cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt)
+        else:
+            region, calpha, abar = prep.cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt, device=device)
         out["pml_region"] = region
         out["pml_coef_alpha"] = calpha.reshape(coords.shape[:4] + (9,))
         out["pml_coef_abar"] = abar.reshape(coords.shape[:4] + (5,))

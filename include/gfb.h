@@ -439,6 +439,44 @@ gfb_status gfb_trainer_get_params(gfb_trainer* trainer, float* params, float* sc
 gfb_status gfb_trainer_set_params(gfb_trainer* trainer, const float* params);
 
 /*
+ * Mesh inputs computed on the device.  The reference computes them on the
+ * host in its Python preprocessor; these produce the same arrays (host
+ * pointers in and out, float64/int32 in the reference layouts) with one GPU
+ * thread per GLL point, processing the cells in bounded chunks.
+ *
+ * gfb_prep_geometry replaces preprocess/gll_geometry.py:132-186 (trilinear
+ * hexes): corners [n_cell][8][3] in GMSH order, GLL points and weights
+ * [ngll] -> coords [n_cell][ngll^3][3], jacobian (det J) [n_cell][ngll^3],
+ * dxi_dx (inv(J) raveled) [n_cell][ngll^3][9], geometric mass
+ * det J w_i w_j w_k [n_cell][ngll^3].
+ */
+gfb_status gfb_prep_geometry(int32_t device, int64_t n_cell, int32_t ngll, const double* gll_x, const double* gll_w,
+                             const double* corners, double* coords, double* jacobian, double* dxi_dx,
+                             double* mass_geo);
+
+/*
+ * Global node numbering, replacing preprocess/partition.py:192-254: points
+ * [n_point][3] quantised to rint(x / (1e-12 extent)), numbered by the
+ * lexicographic (x, y, z) order of the distinct quantised points.
+ * ibool [n_point], n_node = number of distinct points.
+ */
+gfb_status gfb_prep_numbering(int32_t device, int64_t n_point, const double* coords, int32_t* ibool,
+                              int32_t* n_node);
+
+/*
+ * C-PML inputs, replacing preprocess/pml_cpml.py:42-147, 174-253, 261-345,
+ * 353-515: region per cell (0 outside the layer), coef_alpha
+ * [n_cell][ngll^3][9] and A1..A5 abar [n_cell][ngll^3][5] from the points
+ * coords, the cells' PML flags is_pml [n_cell], vp [n_cell][ngll^3], domain
+ * bounds and layer widths (xmin xmax ymin ymax zmin zmax; width 0 = no
+ * layer), the frequency f0 of the alpha profile, dt and log_r = ln R of the
+ * reflection coefficient.
+ */
+gfb_status gfb_prep_cpml(int32_t device, int64_t n_cell, int32_t ngll, const double* coords, const uint8_t* is_pml,
+                         const double* vp, const double* bounds, const double* widths, double f0, double dt,
+                         double log_r, int32_t* region, double* coef_alpha, double* abar);
+
+/*
  * File-level driver: run the forward solve of one direction with the
  * reference's CWD-relative file contract (solver.cpp:73-739,
  * main.cpp:32-137).  Returns 0 on success, 1 on failure, like run_forward.
