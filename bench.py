@@ -542,7 +542,7 @@ def run_reference(args):
         return 0
     import oracle
 
-    prob = build_workload(args.workload)
+    prob = build_workload(args.workload, device=args.device if args.gpu_prep else None)
     which = "ref" if os.path.exists(oracle.LIB_REF) else "oracle"
     threads = os.cpu_count() or 1
     # one direction stands for each of x/y/z: the three reference runs are
@@ -589,7 +589,9 @@ def run_gfb(args):
     device = local if world > 1 else args.device
     prec = gfb.FP32 if args.precision == "fp32" else gfb.FP64
     dirs = [0, 1, 2][: args.fields]
-    prob = build_workload(args.workload)
+    t_gen = time.perf_counter()
+    prob = build_workload(args.workload, device=device if args.gpu_prep else None)
+    t_gen = time.perf_counter() - t_gen
     flags = (gfb.FLAG_RECORD_F32 if args.record_f32 else 0) | (gfb.FLAG_POINT_KERNEL if args.point_kernel else 0)
     s = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8, flags=flags)
     info = s.info()
@@ -670,6 +672,7 @@ def run_gfb(args):
                    "l2": "inputs larger than L2 (geometry alone > 700 MB)", "parallelism": f"replicas{world}",
                    "n_colour": info["n_colour"], "n_pml_cell": info["n_pml_cell"],
                    "elem_blocks": info["elem_blocks"],
+                   "inputs": f"{'GPU (gfb.prep)' if args.gpu_prep else 'host numpy'} generator, {t_gen:.1f} s",
                    "snapshots": f"every {prob['snapshot_stride']} steps, {info['n_rec_cell']} surface cells, "
                                 f"{'float32' if args.record_f32 else 'float64'}, copied to pinned host memory during the step "
                                 f"loop and released by a reader thread"},
@@ -716,6 +719,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 single-direction comparison")
     ap.add_argument("--point-kernel", action="store_true",
                     help="FP32 path with the thread-per-point element kernel instead of the line kernel")
+    ap.add_argument("--gpu-prep", action="store_true",
+                    help="compute the mesh inputs (geometry, numbering, C-PML) on the GPU (gfb.prep)")
     ap.add_argument("--record-f64", dest="record_f32", action="store_false",
                     help="snapshots in double (default: float, the reference example's snapshot_precision)")
     args = ap.parse_args()

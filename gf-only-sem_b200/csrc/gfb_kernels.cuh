@@ -817,8 +817,8 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
 // Pipelining: the geometry of the next group and the node table of the one
 // after are cp.async copies into rotating shared stages; the next group's
 // predicted-displacement vectors are register loads issued one group ahead,
-// this group's old force vectors register loads issued once its gradient
-// phase is done.
+// this group's old force vectors are prefetched into L2 at the start of the
+// group and loaded into registers once its gradient phase is done.
 // ---------------------------------------------------------------------------
 
 // Cells per group of the line kernel: about 150 threads by default; the
@@ -983,6 +983,17 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         if (nx < A.n_groups) issue_geo(nx, (it + 1) & 1);
         if (nx + G < A.n_groups) issue_ib(nx + G, (it + 2) % 3);
         cp_async_commit();
+        // old force vectors of the nodes this colour does not touch first:
+        // start their DRAM reads into L2 now, so the loads issued after the
+        // flux phase find them there (no registers held meanwhile)
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < NG; ++i)
+                if (!(cw[i] & kFirstTouch)) {
+                    const float4* pf = reinterpret_cast<const float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(pf));
+                }
+        }
         const float stf = act ? s_stf[mdl] : 0.f;
         const int src = (act && stf != 0.f && A.src_head) ? __ldg(A.src_head + e) : -1;
         pre_ok = line_nodes(nx, (it + 1) % 3, nw);

@@ -95,25 +95,46 @@ __global__ void geometry_kernel(long long n_cell, int ng, const double* __restri
     const int i = p / (ng * ng), j = (p / ng) % ng, k = p % ng;
     const double xi = gx[i], eta = gx[j], zeta = gx[k];
     const double* X = corners + e * 24;
-    double x[3] = {0.0, 0.0, 0.0};
     double J[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
     for (int a = 0; a < 8; ++a) {
         const double ca = c_corner[a][0], cb = c_corner[a][1], cc = c_corner[a][2];
         const double fa = __dadd_rn(1.0, __dmul_rn(xi, ca));
         const double fb = __dadd_rn(1.0, __dmul_rn(eta, cb));
         const double fc = __dadd_rn(1.0, __dmul_rn(zeta, cc));
-        const double S = __dmul_rn(__dmul_rn(__dmul_rn(0.125, fa), fb), fc);
         const double dS[3] = {__dmul_rn(__dmul_rn(__dmul_rn(0.125, ca), fb), fc),
                               __dmul_rn(__dmul_rn(__dmul_rn(0.125, fa), cb), fc),
                               __dmul_rn(__dmul_rn(__dmul_rn(0.125, fa), fb), cc)};
         for (int c = 0; c < 3; ++c) {
             const double xa = X[a * 3 + c];
-            x[c] = __dadd_rn(x[c], __dmul_rn(S, xa));
             // J[m][c] = sum_a dS[a][m] x_a[c]  (J = dS.T @ corners, gll_geometry.py:173)
             for (int m = 0; m < 3; ++m) J[m][c] = __dadd_rn(J[m][c], __dmul_rn(dS[m], xa));
         }
     }
-    for (int c = 0; c < 3; ++c) coords[t * 3 + c] = x[c];
+    // Coordinates: the same trilinear map evaluated one axis at a time
+    // (along xi between corner pairs, then eta, then zeta).  On a cell face
+    // the weights of the far corners are exactly 0 and 1, so a point shared
+    // by two cells goes through the same rounded operations on the same
+    // corner values in both: bit-identical coordinates, and the quantised
+    // sort cannot split a shared node.  (The one-sum form S @ corners adds
+    // the four face corners in a different order in each cell, and a point
+    // whose copies differ in the last bit can round to two grid values.)
+    const double lw[3] = {__dmul_rn(0.5, __dsub_rn(1.0, xi)), __dmul_rn(0.5, __dsub_rn(1.0, eta)),
+                          __dmul_rn(0.5, __dsub_rn(1.0, zeta))};
+    const double hw[3] = {__dmul_rn(0.5, __dadd_rn(1.0, xi)), __dmul_rn(0.5, __dadd_rn(1.0, eta)),
+                          __dmul_rn(0.5, __dadd_rn(1.0, zeta))};
+    // corner of (xi side, eta side, zeta side) in GMSH order
+    const int cidx[2][2][2] = {{{0, 4}, {3, 7}}, {{1, 5}, {2, 6}}};
+    for (int c = 0; c < 3; ++c) {
+        double s[2];
+        for (int kb = 0; kb < 2; ++kb) {
+            double r[2];
+            for (int jb = 0; jb < 2; ++jb)
+                r[jb] = __dadd_rn(__dmul_rn(lw[0], X[cidx[0][jb][kb] * 3 + c]),
+                                  __dmul_rn(hw[0], X[cidx[1][jb][kb] * 3 + c]));
+            s[kb] = __dadd_rn(__dmul_rn(lw[1], r[0]), __dmul_rn(hw[1], r[1]));
+        }
+        coords[t * 3 + c] = __dadd_rn(__dmul_rn(lw[2], s[0]), __dmul_rn(hw[2], s[1]));
+    }
     const double a = J[0][0], b = J[0][1], c = J[0][2];
     const double d = J[1][0], ee = J[1][1], f = J[1][2];
     const double g = J[2][0], h = J[2][1], ii = J[2][2];

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -111,6 +112,32 @@ void parallel_for(long long n, F&& fn, long long grain = 65536) {
     std::vector<std::thread> th;
     for (unsigned t = 0; t < nt; ++t) th.emplace_back(fn, n * t / nt, n * (t + 1) / nt);
     for (auto& x : th) x.join();
+}
+
+// Append to out, in increasing q, value(q) for every q in [0, n) with
+// keep(q); the host threads count and fill chunks of q in parallel.
+template <typename Keep, typename Value>
+void parallel_compact(long long n, Keep&& keep, Value&& value, std::vector<int>& out) {
+    const long long n_chunk = std::max(1LL, std::min<long long>(256, n / 65536));
+    std::vector<long long> cnt(n_chunk + 1, 0);
+    auto bounds = [&](long long c) { return n * c / n_chunk; };
+    parallel_for(n_chunk, [&](long long c0, long long c1) {
+        for (long long c = c0; c < c1; ++c) {
+            long long k = 0;
+            for (long long q = bounds(c); q < bounds(c + 1); ++q) k += keep(q) ? 1 : 0;
+            cnt[c + 1] = k;
+        }
+    }, 1);
+    for (long long c = 0; c < n_chunk; ++c) cnt[c + 1] += cnt[c];
+    const size_t base = out.size();
+    out.resize(base + (size_t)cnt[n_chunk]);
+    parallel_for(n_chunk, [&](long long c0, long long c1) {
+        for (long long c = c0; c < c1; ++c) {
+            size_t o = base + (size_t)cnt[c];
+            for (long long q = bounds(c); q < bounds(c + 1); ++q)
+                if (keep(q)) out[o++] = value(q);
+        }
+    }, 1);
 }
 
 struct DevBuf {
@@ -267,52 +294,94 @@ gfb_status upload(gfb_solver* s, void** dst, const std::vector<Real>& h) {
     return GFB_OK;
 }
 
-// Pinned staging buffers of staged_upload; the destructor waits for the
-// copies still reading them.
+// Pinned staging buffers of staged_upload: two 64 MB page-locked buffers
+// (portable, so any device's copies may read them), allocated by the first
+// gfb_create that uploads and kept for the rest of the process: pinning and
+// unpinning them on every create cost more than the copies they serve.  The
+// mutex serialises the creates that use them.
 struct Staging {
+    std::mutex mu;
     void* buf[2] = {nullptr, nullptr};
-    cudaEvent_t done[2] = {nullptr, nullptr};
-    ~Staging() {
-        for (int k = 0; k < 2; ++k) {
-            if (done[k]) {
-                cudaEventSynchronize(done[k]);
-                cudaEventDestroy(done[k]);
-            }
-            if (buf[k]) cudaFreeHost(buf[k]);
-        }
-    }
+    size_t bytes = 0;
 };
+Staging& staging() {
+    static Staging* st = new Staging();  // never destroyed: freed with the process
+    return *st;
+}
 
 // Fill the device array dst of n_item items of item_bytes each.  The host
 // threads pack the items chunk by chunk (pack(i0, i1, out) writes items
-// [i0, i1) to out) into two pinned staging buffers in turn, and the copy of
-// one chunk to the device runs while the next is packed: no host copy of the
-// whole array and no copy from pageable memory.
+// [i0, i1) to out) into the two pinned staging buffers in turn, and the copy
+// of one chunk to the device runs while the next is packed: no host copy of
+// the whole array and no copy from pageable memory.  The caller holds
+// staging().mu.
 template <typename Pack>
 gfb_status staged_upload(gfb_solver* s, void* dst, size_t item_bytes, long long n_item, Pack&& pack) {
     if (n_item <= 0) return GFB_OK;
+    Staging& S = staging();
     const size_t stage = size_t(64) << 20;
-    const long long per = std::max<long long>(1, (long long)(stage / item_bytes));
-    const size_t bytes = (size_t)std::min<long long>(per, n_item) * item_bytes;
-    Staging S;
-    for (int k = 0; k < 2; ++k) {
-        CU(cudaHostAlloc(&S.buf[k], bytes, cudaHostAllocDefault));
-        CU(cudaEventCreateWithFlags(&S.done[k], cudaEventDisableTiming));
+    if (S.bytes == 0) {
+        for (int k = 0; k < 2; ++k) CU(cudaHostAlloc(&S.buf[k], stage, cudaHostAllocPortable));
+        S.bytes = stage;
     }
+    struct Events {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~Events() {
+            for (auto x : e)
+                if (x) {
+                    cudaEventSynchronize(x);
+                    cudaEventDestroy(x);
+                }
+        }
+    } done;
+    for (int k = 0; k < 2; ++k) CU(cudaEventCreateWithFlags(&done.e[k], cudaEventDisableTiming));
+    const long long per = std::max<long long>(1, (long long)(S.bytes / item_bytes));
+    if ((size_t)per * item_bytes > S.bytes) return fail(GFB_ERR_UNSUPPORTED, "item of %zu bytes", item_bytes);
     long long c = 0;
     for (long long i0 = 0; i0 < n_item; i0 += per, ++c) {
         const int k = (int)(c & 1);
         const long long i1 = std::min(n_item, i0 + per);
-        CU(cudaEventSynchronize(S.done[k]));  // the copy of chunk c-2 has read the buffer
+        CU(cudaEventSynchronize(done.e[k]));  // the copy of chunk c-2 has read the buffer
         pack(i0, i1, static_cast<unsigned char*>(S.buf[k]));
         CU(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + (size_t)i0 * item_bytes, S.buf[k],
                            (size_t)(i1 - i0) * item_bytes, cudaMemcpyHostToDevice, s->stream));
-        CU(cudaEventRecord(S.done[k], s->stream));
+        CU(cudaEventRecord(done.e[k], s->stream));
     }
     CU(cudaStreamSynchronize(s->stream));
     s->upload_bytes += (long long)((size_t)n_item * item_bytes);
     return GFB_OK;
 }
+
+// The pinned host slots of the snapshot ring, allocated by a helper thread
+// while gfb_create does the rest of its work (page-locking hundreds of MB
+// takes a large part of a second).  finish() hands them over; slots not
+// handed over are freed.
+struct PinnedRing {
+    std::vector<void*> slot;
+    cudaError_t err = cudaSuccess;
+    std::thread worker;
+    bool taken = false;
+    void start(int device, int n, size_t bytes) {
+        slot.assign(n, nullptr);
+        worker = std::thread([this, device, n, bytes] {
+            err = cudaSetDevice(device);
+            for (int k = 0; k < n && err == cudaSuccess; ++k) {
+                err = cudaHostAlloc(&slot[k], bytes, cudaHostAllocDefault);
+                if (err != cudaSuccess) slot[k] = nullptr;
+            }
+        });
+    }
+    cudaError_t finish() {
+        if (worker.joinable()) worker.join();
+        return err;
+    }
+    ~PinnedRing() {
+        if (worker.joinable()) worker.join();
+        if (!taken)
+            for (void* q : slot)
+                if (q) cudaFreeHost(q);
+    }
+};
 
 // Seconds spent in each stage of gfb_create, printed to stderr when the
 // environment variable GFB_TRACE is set.
@@ -760,49 +829,64 @@ bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<dou
         const double* A = m->pml_coef_abar + q * 5;
         return A[0] != 0.0 || A[1] != 0.0 || A[2] != 0.0 || A[3] != 0.0 || A[4] != 0.0;
     };
-    slot.assign(s->n_node, -1);
+    std::vector<int> pcell;
     for (long long e = 0; e < s->n_cell; ++e)
-        if (m->pml_region[e] != 0)
-            for (int p = 0; p < nn; ++p)
-                if (live(e * nn + p)) slot[m->ibool[e * nn + p]] = 0;
+        if (m->pml_region[e] != 0) pcell.push_back((int)e);
+    // each thread owns a range of nodes and visits the C-PML cells in mesh
+    // order, so every node accumulates in the same order as one pass would
+    slot.assign(s->n_node, -1);
+    parallel_for(s->n_node, [&](long long g0, long long g1) {
+        for (int e : pcell)
+            for (int p = 0; p < nn; ++p) {
+                const long long q = (long long)e * nn + p;
+                const int g = m->ibool[q];
+                if (g >= g0 && g < g1 && live(q)) slot[g] = 0;
+            }
+    }, 1 << 18);
     int n = 0;
     for (int g = 0; g < s->n_node; ++g)
         if (slot[g] >= 0) slot[g] = n++;
     coef.assign((size_t)n * 14, 0.0);
     std::vector<unsigned char> have(n, 0);
-    for (long long e = 0; e < s->n_cell; ++e) {
-        if (m->pml_region[e] == 0) continue;
-        for (int p = 0; p < nn; ++p) {
-            const long long q = e * nn + p;
-            if (!live(q)) continue;
-            const double* A = m->pml_coef_abar + q * 5;
-            const int sl = slot[m->ibool[q]];
-            double* c = &coef[(size_t)sl * 14];
-            const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
-            const double wgll = w[ni] * w[nj] * w[nk];
-            const double rho = m->density[q];
-            const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
-            for (int k = 0; k < 5; ++k) c[k] += scale * A[k];
-            const double* al = m->pml_coef_alpha + q * 9;
-            for (int ax = 0; ax < 3; ++ax) {
-                if (A[2 + ax] == 0.0) continue;
-                if (!(have[sl] & (1u << ax))) {
-                    for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
-                    have[sl] |= (unsigned char)(1u << ax);
-                } else {
-                    for (int t = 0; t < 3; ++t) {
-                        const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
-                        // the cells' coefficients at a node come from the same position
-                        // through different cell maps: equal up to rounding (seen up to
-                        // ~1e-9 relative on deformed meshes); different profiles differ
-                        // at O(1)
-                        if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) return false;
+    std::atomic<bool> agree(true);
+    parallel_for(s->n_node, [&](long long g0, long long g1) {
+        for (int e : pcell) {
+            for (int p = 0; p < nn; ++p) {
+                const long long q = (long long)e * nn + p;
+                const int g = m->ibool[q];
+                if (g < g0 || g >= g1 || !live(q)) continue;
+                const double* A = m->pml_coef_abar + q * 5;
+                const int sl = slot[g];
+                double* c = &coef[(size_t)sl * 14];
+                const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
+                const double wgll = w[ni] * w[nj] * w[nk];
+                const double rho = m->density[q];
+                const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
+                for (int k = 0; k < 5; ++k) c[k] += scale * A[k];
+                const double* al = m->pml_coef_alpha + q * 9;
+                for (int ax = 0; ax < 3; ++ax) {
+                    if (A[2 + ax] == 0.0) continue;
+                    if (!(have[sl] & (1u << ax))) {
+                        for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
+                        have[sl] |= (unsigned char)(1u << ax);
+                    } else {
+                        for (int t = 0; t < 3; ++t) {
+                            const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
+                            // the cells' coefficients at a node come from the same position
+                            // through different cell maps: equal up to rounding (seen up to
+                            // ~1e-9 relative on deformed meshes); different profiles differ
+                            // at O(1)
+                            if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) {
+                                agree.store(false);
+                                return;
+                            }
+                        }
                     }
                 }
             }
         }
-    }
-    return true;
+    }, 1 << 18);
+    return agree.load();
 }
 
 // Upload the node-form C-PML: the C-PML nodes are device nodes [0, n)
@@ -832,11 +916,44 @@ template <typename Real>
 gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src, int n_model,
                         const gfb_model* models, const std::vector<int>& perm, const std::vector<int>& inv_perm,
                         const std::vector<uint32_t>& ibool_dev, const std::vector<double>& node_mass,
-                        const std::vector<double>& node_damp, const std::vector<double>& w,
-                        const std::vector<double>& D, StageClock& clk) {
+                        const std::vector<double>& node_damp, const std::vector<long long>& first_q,
+                        const std::vector<double>& w, const std::vector<double>& D, StageClock& clk) {
     const int ng = s->ng, nn = s->nn;
     const long long n_cell = s->n_cell;
     gfb_status st;
+    std::lock_guard<std::mutex> staging_lock(staging().mu);
+    PinnedRing host_ring;
+    // recording nodes: unique node ids in ascending order (the recording
+    // map's gll_node_ids), each node's (cell, point) occurrences, and the
+    // mass of each occurrence as the merge weight
+    if (s->n_rec > 0) {
+        std::vector<std::pair<int, int>> occ;  // (node, record index)
+        occ.reserve((size_t)s->n_rec * nn);
+        for (int ci = 0; ci < s->n_rec; ++ci)
+            for (int p = 0; p < nn; ++p)
+                occ.push_back({m->ibool[(size_t)m->rec_cell_local[ci] * nn + p], ci * nn + p});
+        std::sort(occ.begin(), occ.end());
+        std::vector<int> ptr{0}, idx;
+        std::vector<double> wts;
+        s->rec_node_ids.clear();
+        for (size_t k = 0; k < occ.size(); ++k) {
+            if (k == 0 || occ[k].first != occ[k - 1].first) {
+                if (k) ptr.push_back((int)k);
+                s->rec_node_ids.push_back(occ[k].first);
+            }
+            idx.push_back(occ[k].second);
+            const int ci = occ[k].second / nn, p = occ[k].second - ci * nn;
+            wts.push_back(m->mass[(size_t)m->rec_cell_local[ci] * nn + p]);
+        }
+        ptr.push_back((int)occ.size());
+        s->n_unique = (int)s->rec_node_ids.size();
+        if ((st = s->alloc(&s->gf_ptr, ptr.size())) || (st = h2d(s, s->gf_ptr, ptr.data(), ptr.size() * 4))) return st;
+        if ((st = s->alloc(&s->gf_occ, idx.size())) || (st = h2d(s, s->gf_occ, idx.data(), idx.size() * 4))) return st;
+        if ((st = s->alloc(&s->gf_w, wts.size())) || (st = h2d(s, s->gf_w, wts.data(), wts.size() * 8))) return st;
+    }
+    // the snapshot size is known now: pin the host ring meanwhile
+    if (s->n_rec > 0) host_ring.start(s->device, s->slots, snapshot_bytes(s));
+    clk.mark("recording nodes");
     // C-PML at global nodes (FP32 path) when the cells agree at shared nodes.
     // Device node order: the node-form C-PML nodes first (so they are device
     // nodes [0, n_pml_node)), then the others; within each, nodes in the
@@ -848,37 +965,48 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     std::vector<double> pcoef;
     const bool node_form = s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML) &&
                            plan_node_pml(s, m, w, pslot, pcoef);
+    clk.mark("C-PML node plan");
     {
+        // a point q is its node's first touch when first_q[node] == q
         s->node_perm.clear();
         s->node_inv.clear();
         s->node_perm.reserve(s->n_node);
-        std::vector<char> seen(s->n_node, 0);
+        const long long P = n_cell * nn;
+        auto node_of = [&](long long q) { return m->ibool[q]; };
         for (int pass = node_form ? 0 : 1; pass < 2; ++pass)
-            for (long long q = 0; q < n_cell * nn; ++q) {
+            parallel_compact(P, [&](long long q) {
                 const int g = m->ibool[q];
-                if (seen[g] || (pass == 0 && pslot[g] < 0)) continue;
-                seen[g] = 1;
-                s->node_perm.push_back(g);
-            }
-        for (int g = 0; g < s->n_node; ++g)  // nodes no cell uses
-            if (!seen[g]) s->node_perm.push_back(g);
-        bool ident = true;
-        for (int d = 0; d < s->n_node && ident; ++d) ident = s->node_perm[d] == d;
-        if (ident) {
+                return first_q[g] == q && (pass == 1 ? (!node_form || pslot[g] < 0) : pslot[g] >= 0);
+            }, node_of, s->node_perm);
+        parallel_compact(s->n_node, [&](long long g) { return first_q[g] < 0; },  // nodes no cell uses
+                         [](long long g) { return (int)g; }, s->node_perm);
+        std::atomic<bool> ident(true);
+        parallel_for(s->n_node, [&](long long d0, long long d1) {
+            for (long long d = d0; d < d1; ++d)
+                if (s->node_perm[d] != (int)d) {
+                    ident.store(false);
+                    return;
+                }
+        });
+        if (ident.load()) {
             s->node_perm.clear();
         } else {
             s->node_inv.assign(s->n_node, 0);
-            for (int d = 0; d < s->n_node; ++d) s->node_inv[s->node_perm[d]] = d;
+            parallel_for(s->n_node, [&](long long d0, long long d1) {
+                for (long long d = d0; d < d1; ++d) s->node_inv[s->node_perm[d]] = (int)d;
+            });
         }
         if (node_form) {
             // slots follow the device order
             const int n_slot = (int)(pcoef.size() / 14);
             std::vector<double> c2(pcoef.size());
-            for (int d = 0; d < n_slot; ++d) {
-                const int g = s->node_perm.empty() ? d : s->node_perm[d];
-                std::copy(pcoef.begin() + (size_t)pslot[g] * 14, pcoef.begin() + (size_t)pslot[g] * 14 + 14,
-                          c2.begin() + (size_t)d * 14);
-            }
+            parallel_for(n_slot, [&](long long d0, long long d1) {
+                for (long long d = d0; d < d1; ++d) {
+                    const int g = s->node_perm.empty() ? (int)d : s->node_perm[d];
+                    std::copy(pcoef.begin() + (size_t)pslot[g] * 14, pcoef.begin() + (size_t)pslot[g] * 14 + 14,
+                              c2.begin() + (size_t)d * 14);
+                }
+            });
             pcoef.swap(c2);
         }
     }
@@ -887,7 +1015,9 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     auto permuted = [&](const std::vector<double>& h) {
         if (s->node_perm.empty()) return h;
         std::vector<double> o(h.size());
-        for (size_t d = 0; d < o.size(); ++d) o[d] = h[s->node_perm[d]];
+        parallel_for((long long)o.size(), [&](long long d0, long long d1) {
+            for (long long d = d0; d < d1; ++d) o[d] = h[s->node_perm[d]];
+        });
         return o;
     };
     // ibool in device node numbers, and the rows of the pipelined kernels:
@@ -978,6 +1108,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     CU(cudaMemset(a, 0, nF * sizeof(Real)));
     CU(cudaMemset(ut, 0, nP * sizeof(Real)));
     CU(cudaMemset(force, 0, nP * sizeof(Real)));
+    clk.mark("state arrays");
     const std::vector<double> mass_d = permuted(node_mass);
     {
         double* d = nullptr;
@@ -997,6 +1128,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         if ((st = h2d(s, d, damp_d.data(), damp_d.size() * 8))) return st;
         s->damping = d;
     }
+    clk.mark("mass and damping");
     if (node_form && (st = upload_node_pml<Real>(s, pcoef))) return st;
     // C-PML per cell
     if (s->has_cpml && !s->node_pml) {
@@ -1045,6 +1177,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         s->pml_mem = mem;
         s->pml_prev = prev;
     }
+    clk.mark("C-PML arrays");
     // source: cells located by id (solver.cpp:250-258), chained per cell
     if (src && src->n_src_cell > 0) {
         std::vector<int> head(n_cell, -1), next(src->n_src_cell, -1), tail(n_cell, -1);
@@ -1078,6 +1211,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         s->src_next = dn;
         if ((st = upload(s, &s->src_w, wts))) return st;
     }
+    clk.mark("source");
     // models: constants, step counters, source time functions
     {
         std::vector<gfb::ModelConst> mc(n_model);
@@ -1122,34 +1256,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         s->n_pml = 0;
         for (long long e = 0; e < n_cell; ++e) s->n_pml += m->pml_region[e] != 0;
     }
-    // recording nodes: unique node ids in ascending order (the recording
-    // map's gll_node_ids), each node's (cell, point) occurrences, and the
-    // mass of each occurrence as the merge weight
-    if (s->n_rec > 0) {
-        std::vector<std::pair<int, int>> occ;  // (node, record index)
-        occ.reserve((size_t)s->n_rec * nn);
-        for (int ci = 0; ci < s->n_rec; ++ci)
-            for (int p = 0; p < nn; ++p)
-                occ.push_back({m->ibool[(size_t)m->rec_cell_local[ci] * nn + p], ci * nn + p});
-        std::sort(occ.begin(), occ.end());
-        std::vector<int> ptr{0}, idx;
-        std::vector<double> wts;
-        s->rec_node_ids.clear();
-        for (size_t k = 0; k < occ.size(); ++k) {
-            if (k == 0 || occ[k].first != occ[k - 1].first) {
-                if (k) ptr.push_back((int)k);
-                s->rec_node_ids.push_back(occ[k].first);
-            }
-            idx.push_back(occ[k].second);
-            const int ci = occ[k].second / nn, p = occ[k].second - ci * nn;
-            wts.push_back(m->mass[(size_t)m->rec_cell_local[ci] * nn + p]);
-        }
-        ptr.push_back((int)occ.size());
-        s->n_unique = (int)s->rec_node_ids.size();
-        if ((st = s->alloc(&s->gf_ptr, ptr.size())) || (st = h2d(s, s->gf_ptr, ptr.data(), ptr.size() * 4))) return st;
-        if ((st = s->alloc(&s->gf_occ, idx.size())) || (st = h2d(s, s->gf_occ, idx.data(), idx.size() * 4))) return st;
-        if ((st = s->alloc(&s->gf_w, wts.size())) || (st = h2d(s, s->gf_w, wts.data(), wts.size() * 8))) return st;
-    }
+    clk.mark("models");
     // recording cells and snapshot ring
     if (s->n_rec > 0) {
         std::vector<int> rc(s->n_rec);
@@ -1161,16 +1268,18 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         unsigned char* ring = nullptr;
         if ((st = s->alloc(&ring, snapshot_bytes(s) * s->slots))) return st;
         s->ring = ring;
-        s->pinned.assign(s->slots, nullptr);
         s->rec_evt.assign(s->slots, nullptr);
         s->copy_evt.assign(s->slots, nullptr);
         s->copy_issued.assign(s->slots, 0);
         for (int k = 0; k < s->slots; ++k) {
-            CU(cudaHostAlloc(&s->pinned[k], snapshot_bytes(s), cudaHostAllocDefault));
             CU(cudaEventCreateWithFlags(&s->rec_evt[k], cudaEventDisableTiming));
             CU(cudaEventCreateWithFlags(&s->copy_evt[k], cudaEventDisableTiming));
         }
+        CU(host_ring.finish());
+        s->pinned = host_ring.slot;  // the solver frees them from here on
+        host_ring.taken = true;
     }
+    clk.mark("snapshot ring");
     return GFB_OK;
 }
 
@@ -1346,6 +1455,27 @@ const char* gfb_last_error(void) { return g_err.c_str(); }
 
 namespace {
 
+// Greedy colouring of the cells in mesh order with a colour mask of T per
+// node; false when some cell would need a colour beyond T's width.
+template <typename T>
+bool greedy_colour(const gfb_mesh* m, int nn, std::vector<T>& used, std::vector<int>& colour, int& n_colour) {
+    used.assign(m->n_node, T(0));
+    n_colour = 0;
+    for (long long e = 0; e < m->n_cell; ++e) {
+        T u = 0;
+        const int* ib = m->ibool + e * nn;
+        for (int p = 0; p < nn; ++p) u |= used[ib[p]];
+        const T avail = (T)~u;
+        if (avail == 0) return false;
+        const int col = __builtin_ctzll((unsigned long long)avail);
+        colour[e] = col;
+        n_colour = std::max(n_colour, col + 1);
+        const T bit = (T)((T)1 << col);
+        for (int p = 0; p < nn; ++p) used[ib[p]] |= bit;
+    }
+    return true;
+}
+
 gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, int n_model,
                        const gfb_model* models, gfb_solver** out) {
     gfb_status st;
@@ -1426,13 +1556,17 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     // global lumped mass (accumulate) and damping (assign), solver.cpp:193-202.
     // Each thread owns a range of nodes and scans every entry in mesh order,
     // so every node sums (and assigns) in the reference's order
+    // The same pass records each node's first touch (the first point in
+    // mesh order that lists it), from which the device numbering follows.
     std::vector<double> node_mass(m->n_node, 0.0), node_damp(m->n_node, 0.0);
+    std::vector<long long> first_q(m->n_node, -1);
     parallel_for(m->n_node, [&](long long g0, long long g1) {
         for (long long q = 0; q < P; ++q) {
             const int g = m->ibool[q];
             if (g < g0 || g >= g1) continue;
             node_mass[g] += m->mass[q];
             node_damp[g] = m->damping ? m->damping[q] : 0.0;
+            if (first_q[g] < 0) first_q[g] = q;
         }
     }, 1 << 18);
     clk.mark("lumped mass");
@@ -1444,19 +1578,21 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
                 break;
             }
     // greedy colouring in cell order: colour = lowest colour unused by any
-    // cell already sharing a node (structured meshes get the 8 parity colours)
-    std::vector<uint64_t> used(m->n_node, 0);
+    // cell already sharing a node (structured meshes get the 8 parity
+    // colours).  Byte masks per node first (an eighth of the memory
+    // traffic); a mesh that needs a ninth colour is coloured again with
+    // 64-bit masks, which gives the same colours
+    std::vector<uint8_t> used8;
+    std::vector<uint64_t> used64;
     std::vector<int> colour(m->n_cell);
     int n_colour = 0;
-    for (long long e = 0; e < m->n_cell; ++e) {
-        uint64_t u = 0;
-        for (int p = 0; p < nn; ++p) u |= used[m->ibool[e * nn + p]];
-        if (~u == 0) return fail(GFB_ERR_UNSUPPORTED, "mesh needs more than 64 colours");
-        const int col = __builtin_ctzll(~u);
-        colour[e] = col;
-        n_colour = std::max(n_colour, col + 1);
-        for (int p = 0; p < nn; ++p) used[m->ibool[e * nn + p]] |= (1ull << col);
+    const bool narrow = greedy_colour(m, nn, used8, colour, n_colour);
+    if (!narrow) {
+        std::vector<uint8_t>().swap(used8);
+        if (!greedy_colour(m, nn, used64, colour, n_colour))
+            return fail(GFB_ERR_UNSUPPORTED, "mesh needs more than 64 colours");
     }
+    auto used_mask = [&](uint32_t g) -> uint64_t { return narrow ? (uint64_t)used8[g] : used64[g]; };
     clk.mark("colouring");
     std::vector<int> perm(m->n_cell), inv_perm(m->n_cell);
     s->colour_begin.assign(n_colour + 1, 0);
@@ -1479,8 +1615,9 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
             const long long e = perm[ed];
             for (int p = 0; p < nn; ++p) {
                 const uint32_t g = (uint32_t)m->ibool[e * nn + p];
-                const bool first = __builtin_ctzll(used[g]) == colour[e];
-                const bool last = 63 - __builtin_clzll(used[g]) == colour[e];
+                const uint64_t um = used_mask(g);
+                const bool first = __builtin_ctzll(um) == colour[e];
+                const bool last = 63 - __builtin_clzll(um) == colour[e];
                 ibool_dev[ed * nn + p] = g | (first ? gfb::kFirstTouch : 0u) | (last ? gfb::kLastTouch : 0u);
             }
         }
@@ -1491,11 +1628,11 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     if (s->prec == GFB_FP64) {
         if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<double>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                  w, D, clk);
+                                  first_q, w, D, clk);
     } else {
         if ((st = dispatch<float, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<float>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                 w, D, clk);
+                                 first_q, w, D, clk);
     }
     if (st) return st;
     CU(cudaStreamSynchronize(s->stream));
