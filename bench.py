@@ -683,7 +683,9 @@ def run_gfb(args):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "kernel": f"{kname} (all colour launches of a step)",
                      "algorithmic_bytes_per_step": eb,
-                     "traffic": (traffic or {}).get("bytes_per_step") if traffic else None},
+                     "traffic": (traffic["bytes_per_cell"] * prob["n_cell"]
+                                 if traffic and prec == gfb.FP32 and not args.point_kernel else None),
+                     "traffic_source": (traffic or {}).get("source") if traffic else None},
         "roofline_node": {"achieved": nb / (ms_node / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                           "algorithmic_bytes_per_step": nb},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": up / args.steps,
