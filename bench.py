@@ -42,14 +42,14 @@ for _p in (REPO, PKG):
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
-    # layered model, three directions batched
+    # layered model, 64 x 64 x 32 cells, three directions batched
     "layered_64x64x32": dict(nx=64, ny=64, nz=32, d=250.0, pml=4, seed=2, src=(8000.0, 8000.0, 2000.0),
                              nsteps=4000, stride=10, depth=250.0),
     # the same model at 40 x 40 x 20 cells: inputs still larger than L2 but
     # about 1 GB on the device, for ncu captures
     "layered_40x40x20": dict(nx=40, ny=40, nz=20, d=400.0, pml=4, seed=2, src=(8000.0, 8000.0, 2000.0),
                              nsteps=2500, stride=10, depth=400.0),
-    # deformed heterogeneous mesh (jittered interior vertices,
+    # deformed heterogeneous mesh, 128 x 128 x 64 cells (jittered interior vertices,
     # 8-sinusoid topography, Gaussian-correlated velocity perturbation),
     # strain Green's functions recorded on a 16 x 16-element tile
     "deformed_128x128x64": dict(nx=128, ny=128, nz=64, d=200.0, pml=5, seed=3, src=(12800.0, 12800.0, 2000.0),
@@ -59,17 +59,17 @@ WORKLOADS = {
     "deformed_32x32x16": dict(nx=32, ny=32, nz=16, d=200.0, pml=5, seed=3, src=(3200.0, 3200.0, 1400.0),
                               nsteps=1500, stride=10, depth=200.0, jitter=0.1, topo=(8, 300.0), corr=150.0,
                               pert=0.1, tile=8),
-    # configs[0]-shaped halfspace (CPU-runnable size) for quick runs
+    # homogeneous halfspace at a CPU-runnable size (20 x 20 x 10) for quick runs
     "halfspace_20x20x10": dict(nx=20, ny=20, nz=10, d=500.0, pml=3, seed=0, src=(5000.0, 5000.0, 1000.0),
                                nsteps=2000, stride=10, depth=500.0),
 }
 
-# configs[3]: 32 independent models of uneven size stepped together
+# 32 independent models of uneven size stepped together
 BATCH = dict(n_model=32, seed=4, d=250.0, pml=4, nmin=(16, 16, 8), nmax=(48, 48, 24), f0=(1.0, 3.0),
              steps=(1000, 3000), stride=50)
 
-# configs[4]: learned one-element absorbing layer on a 96 x 96 x 48 layered
-# model (interior 94 x 94 x 47), judged against the same interior with a
+# learned one-element absorbing layer on a 96 x 96 x 48 layered
+# model (interior 94 x 94 x 47), scored against the same interior with a
 # 10-element C-PML; networks trained on replays of small seeded models
 LAYER = {
     "layer96": dict(ni=94, nk=47, d=250.0, seed=2, steps=2000, stride=50,
@@ -236,8 +236,8 @@ def run_layer(args):
     samples = int(tr.samples().sum())
     tr.close()
 
-    # the evaluation model: the thick judge first, then (with the thick
-    # problem freed) the thin domain at the same time step
+    # the evaluation model: the thick-C-PML reference first, then (with the
+    # thick problem freed) the thin domain at the same time step
     p = pair(w["seed"], w["ni"], w["nk"], w["steps"], w["stride"])
     thick = gl.build_domain(p, p.n_thick)
     shift = (p.n_thick - p.n_thin) * d
@@ -247,7 +247,7 @@ def run_layer(args):
                        flags=gfb.FLAG_RECORD_F32)
         if learned:
             gl.attach(s, gl.Layer(prob), params, scales, threshold=0.05)
-        # only the recorded displacement is kept (float32): the judge's
+        # only the recorded displacement is kept (float32): the compared
         # quantity, and small enough for 96 x 96 surface cells
         import ctypes as C
 
@@ -275,7 +275,7 @@ def run_layer(args):
         snaps = {f: {"u": np.stack(us[f])} for f in range(3)}
         return snaps, ms / w["steps"], st
 
-    judge, ms_thick, _ = run(thick, False)
+    thick_rec, ms_thick, _ = run(thick, False)
     thick_keys, thick_cells, dt = gl.surface_keys(thick), thick["n_cell"], thick["dt"]
     del thick
     thin = gl.build_domain(p, p.n_thin, dt)
@@ -285,9 +285,9 @@ def run_layer(args):
     params = params * 0.0  # the same layer untrained: constant damping softplus(0) on every axis
     untrained, _, _ = run(thin, True)
     params = trained
-    err_plain = [gl.reflection_error(thin, plain[f], thick_keys, judge[f], shift) for f in range(3)]
-    err_learned = [gl.reflection_error(thin, learned[f], thick_keys, judge[f], shift) for f in range(3)]
-    err_untrained = [gl.reflection_error(thin, untrained[f], thick_keys, judge[f], shift) for f in range(3)]
+    err_plain = [gl.reflection_error(thin, plain[f], thick_keys, thick_rec[f], shift) for f in range(3)]
+    err_learned = [gl.reflection_error(thin, learned[f], thick_keys, thick_rec[f], shift) for f in range(3)]
+    err_untrained = [gl.reflection_error(thin, untrained[f], thick_keys, thick_rec[f], shift) for f in range(3)]
     value = float(np.sqrt(np.mean(np.square(err_learned))))
     line = {
         "metric": "reflection error of a learned 1-element absorbing layer vs a 10-element C-PML "

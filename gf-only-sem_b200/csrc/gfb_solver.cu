@@ -2164,7 +2164,7 @@ int32_t gfb_run_forward(const char* direction, int32_t resume, int32_t effective
         fail(GFB_ERR_INVALID, "--direction must be x, y, or z");
         return 1;
     }
-    fail(GFB_ERR_IO, "this build has no HDF5 reader for config.h5 / partition_{r}.h5");
+    fail(GFB_ERR_IO, "the library was built without an HDF5 reader for config.h5 / partition_{r}.h5");
     return 1;
 }
 

@@ -6,7 +6,7 @@ element C-PML on the five absorbing faces (x-, x+, y-, y+ and the bottom;
 the top is the free surface) and *thin* with a one-element C-PML.  The thin
 domain's layer nodes get a force correction from one network per node class
 (side or bottom face x depth plane inside the layer cell); the networks are
-trained so that the thin run follows the thick run, which is also the judge
+trained so that the thin run follows the thick run, which is also the reference
 of the reflection error.
 """
 
@@ -312,7 +312,7 @@ def collect_pair(trainer: Trainer, p: PairSpec, dirs=(0, 1, 2), n_steps: Optiona
 
 
 # ---------------------------------------------------------------------------
-# evaluation against the thick-C-PML judge
+# evaluation against the thick-C-PML reference run
 # ---------------------------------------------------------------------------
 
 def surface_records(prob: dict, snaps: dict, shift: float):

@@ -221,7 +221,7 @@ def gl_split(p):
 def test_trained_layer_reduces_reflection_against_thick_cpml():
     """End to end on small models: collect replays of two seeded pairs, fit,
     then the reflection error of the thin domain (one-element C-PML) with the
-    trained layer against the 10-element C-PML judge, on a held-out model,
+    trained layer against the 10-element C-PML reference run, on a held-out model,
     is well below that of the same thin domain without the layer."""
     def pair(seed, steps):
         r = np.random.default_rng(seed)
@@ -253,10 +253,10 @@ def test_trained_layer_reduces_reflection_against_thick_cpml():
         s.close()
         return out, st
 
-    judge, _ = run(thick, False)
+    thick_rec, _ = run(thick, False)
     plain, _ = run(thin, False)
     learned, st = run(thin, True)
     assert st[0]  # still active: no fallback was needed
-    e_plain = gl.reflection_error(thin, plain, thick, judge, shift)
-    e_learned = gl.reflection_error(thin, learned, thick, judge, shift)
+    e_plain = gl.reflection_error(thin, plain, thick, thick_rec, shift)
+    e_learned = gl.reflection_error(thin, learned, thick, thick_rec, shift)
     assert e_learned < 0.7 * e_plain, (e_learned, e_plain)
