@@ -73,9 +73,11 @@ BATCH = dict(n_model=32, seed=4, d=250.0, pml=4, nmin=(16, 16, 8), nmax=(48, 48,
 # 10-element C-PML; networks trained on replays of small seeded models
 LAYER = {
     "layer96": dict(ni=94, nk=47, d=250.0, seed=2, steps=2000, stride=50,
-                    train_pairs=24, train_ni=10, train_nk=6, train_steps=700, epochs=30),
+                    train_pairs=24, train_ni=10, train_nk=6, train_steps=700, epochs=30,
+                    val_ni=22, val_nk=11, val_steps=900),
     "layer24": dict(ni=22, nk=11, d=250.0, seed=2, steps=900, stride=10,
-                    train_pairs=6, train_ni=8, train_nk=5, train_steps=500, epochs=15),
+                    train_pairs=6, train_ni=8, train_nk=5, train_steps=500, epochs=15,
+                    val_ni=16, val_nk=8, val_steps=600),
 }
 
 METRIC = "GLL-point updates/s (FP32 batched x/y/z, 1 B200)"
@@ -236,21 +238,19 @@ def run_layer(args):
     samples = int(tr.samples().sum())
     tr.close()
 
-    # the evaluation model: the thick-C-PML reference first, then (with the
-    # thick problem freed) the thin domain at the same time step
-    p = pair(w["seed"], w["ni"], w["nk"], w["steps"], w["stride"])
-    thick = gl.build_domain(p, p.n_thick)
-    shift = (p.n_thick - p.n_thin) * d
-
-    def run(prob, learned):
-        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, device=args.device, record_slots=16,
-                       flags=gfb.FLAG_RECORD_F32)
-        if learned:
-            gl.attach(s, gl.Layer(prob), params, scales, threshold=0.05)
-        # only the recorded displacement is kept (float32): the compared
-        # quantity, and small enough for 96 x 96 surface cells
+    def run(prob, weights=None, scale_mult=1.0, n_steps=None):
+        """Step prob (with the layer when weights are given, its output scale
+        times scale_mult) and keep the recorded displacement (float32: the
+        compared quantity, and small enough for 96 x 96 surface cells)."""
         import ctypes as C
 
+        n_steps = n_steps or int(prob["nsteps"])
+        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, device=args.device, record_slots=16,
+                       flags=gfb.FLAG_RECORD_F32)
+        if weights is not None:
+            sc = np.array(scales, dtype=np.float32)
+            sc[3] *= scale_mult
+            gl.attach(s, gl.Layer(prob), weights, sc, threshold=0.05)
         us = {f: [] for f in range(3)}
         step = C.c_int32()
         null = C.cast(None, C.POINTER(C.c_double))
@@ -265,30 +265,69 @@ def run_layer(args):
 
         ms = 0.0
         done = 0
-        while done < w["steps"]:
-            k = min(200, w["steps"] - done)
+        while done < n_steps:
+            k = min(200, n_steps - done)
             ms += s.advance_timed(k)
             read_all()
             done += k
-        st = gl.status(s) if learned else None
+        st = gl.status(s) if weights is not None else None
         s.close()
         snaps = {f: {"u": np.stack(us[f])} for f in range(3)}
-        return snaps, ms / w["steps"], st
+        return snaps, ms / n_steps, st
 
-    thick_rec, ms_thick, _ = run(thick, False)
+    def rms(x):
+        return float(np.sqrt(np.mean(np.square(x))))
+
+    # closed-loop selection on held-out models: the one-step replay loss the
+    # networks are fitted to is not the reflection error, so the candidates
+    # (trained or untrained weights, output scale x 0.25 .. 4) are compared
+    # by the reflection error they give when stepping two validation models
+    # (seeds of neither the training nor the test model), and the best is
+    # the layer that goes to the test model
+    zero = params * 0.0  # untrained: constant damping softplus(0) on every axis
+    t0 = time.perf_counter()
+    val = []
+    for vseed in (5000, 5001):
+        pv = pair(vseed, w["val_ni"], w["val_nk"], w["val_steps"], 10)
+        thv = gl.build_domain(pv, pv.n_thick)
+        thv_rec, _, _ = run(thv)
+        keys, dtv = gl.surface_keys(thv), thv["dt"]
+        del thv
+        val.append((pv, gl.build_domain(pv, pv.n_thin, dtv), keys, thv_rec))
+    cands = [(wname, wts, k) for wname, wts in (("trained", params), ("untrained", zero))
+             for k in (0.25, 0.5, 1.0, 2.0, 4.0)]
+    scores = []
+    for wname, wts, k in cands:
+        errs = []
+        for pv, tn, keys, thv_rec in val:
+            rec, _, _ = run(tn, wts, k)
+            errs += [gl.reflection_error(tn, rec[f], keys, thv_rec[f], (pv.n_thick - pv.n_thin) * d)
+                     for f in range(3)]
+        scores.append(rms(errs))
+    best = int(np.argmin(scores))
+    sel_name, sel_w, sel_k = cands[best]
+    t_select = time.perf_counter() - t0
+    del val
+
+    # the test model: the thick-C-PML reference first, then (with the thick
+    # problem freed) the thin domain at the same time step
+    p = pair(w["seed"], w["ni"], w["nk"], w["steps"], w["stride"])
+    thick = gl.build_domain(p, p.n_thick)
+    shift = (p.n_thick - p.n_thin) * d
+    thick_rec, ms_thick, _ = run(thick)
     thick_keys, thick_cells, dt = gl.surface_keys(thick), thick["n_cell"], thick["dt"]
     del thick
     thin = gl.build_domain(p, p.n_thin, dt)
-    plain, ms_plain, _ = run(thin, False)
-    learned, ms_learned, st = run(thin, True)
-    trained = params
-    params = params * 0.0  # the same layer untrained: constant damping softplus(0) on every axis
-    untrained, _, _ = run(thin, True)
-    params = trained
-    err_plain = [gl.reflection_error(thin, plain[f], thick_keys, thick_rec[f], shift) for f in range(3)]
-    err_learned = [gl.reflection_error(thin, learned[f], thick_keys, thick_rec[f], shift) for f in range(3)]
-    err_untrained = [gl.reflection_error(thin, untrained[f], thick_keys, thick_rec[f], shift) for f in range(3)]
-    value = float(np.sqrt(np.mean(np.square(err_learned))))
+    plain, ms_plain, _ = run(thin)
+    selected, ms_learned, st = run(thin, sel_w, sel_k)
+    trained_k1, _, _ = run(thin, params, 1.0)
+    untrained, _, _ = run(thin, zero, 1.0)
+
+    def errs_of(snaps):
+        return [gl.reflection_error(thin, snaps[f], thick_keys, thick_rec[f], shift) for f in range(3)]
+
+    err_plain, err_sel, err_trained, err_untrained = (errs_of(x) for x in (plain, selected, trained_k1, untrained))
+    value = rms(err_sel)
     line = {
         "metric": "reflection error of a learned 1-element absorbing layer vs a 10-element C-PML "
                   "(rel L2 of recorded surface displacement, x/y/z)",
@@ -300,8 +339,13 @@ def run_layer(args):
                    "train_pairs": w["train_pairs"], "train_samples": samples, "epochs": w["epochs"],
                    "loss_zero_prediction": base, "loss_first_epoch": float(loss[0]) if len(loss) else None,
                    "loss_last_epoch": float(loss[-1]) if len(loss) else None,
-                   "collect_s": t_collect, "fit_s": t_fit},
-        "reflection_error": {"learned": err_learned, "thin_cpml_only": err_plain,
+                   "collect_s": t_collect, "fit_s": t_fit, "select_s": t_select},
+        "selection": {"on": f"2 held-out models {w['val_ni']}x{w['val_ni']}x{w['val_nk']} cells, "
+                            f"{w['val_steps']} steps",
+                      "chosen": {"weights": sel_name, "output_scale_x": sel_k},
+                      "validation_error": {f"{c[0]} x{c[2]}": sc for c, sc in zip(cands, scores)}},
+        "reflection_error": {"learned_selected": err_sel, "thin_cpml_only": err_plain,
+                             "trained_network_scale_x1": err_trained,
                              "untrained_network_constant_damping": err_untrained},
         "ms_per_step": {"thick_cpml": ms_thick, "thin_cpml_only": ms_plain, "thin_learned": ms_learned},
         "layer_active_at_end": bool(st[0]) if st else None, "monitored_residual": st[1] if st else None,
@@ -722,12 +766,22 @@ def main():
     ap.add_argument("--point-kernel", action="store_true",
                     help="FP32 path with the thread-per-point element kernel instead of the line kernel")
     ap.add_argument("--gpu-prep", action="store_true",
-                    help="compute the mesh inputs (geometry, numbering, C-PML) on the GPU (gfb.prep)")
+                    help="compute the mesh inputs (geometry, numbering, C-PML) on the GPU (gfb.prep); "
+                         "the default for the deformed workloads")
+    ap.add_argument("--host-prep", action="store_true",
+                    help="compute every mesh input with the host generator (the reference's arithmetic, "
+                         "including the nodes its numbering splits on deformed meshes)")
     ap.add_argument("--record-f64", dest="record_f32", action="store_false",
                     help="snapshots in double (default: float, the reference example's snapshot_precision)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    # deformed meshes: the host generator's numbering splits some shared
+    # nodes (524 on 128 x 128 x 64), the GPU generator none
+    if args.workload.startswith("deformed") and not args.host_prep:
+        args.gpu_prep = True
+    if args.host_prep:
+        args.gpu_prep = False
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch32":
