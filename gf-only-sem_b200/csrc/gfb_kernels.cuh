@@ -82,6 +82,7 @@ struct NodeArgs {
     const uint8_t* node_model;
     const ModelConst* mc;
     const int* mlive;
+    const long long* live_node_end;  // [2] end of the stepping C-PML / plain nodes (several models), or null
 };
 
 // C-PML at global nodes (FP32 path).
@@ -441,7 +442,8 @@ __device__ __forceinline__ bool node_constants(const NodeArgs<Real>& A, const No
 
 template <typename Real, int NFLD, bool MULTI>
 __global__ void __launch_bounds__(256, 3) node_update_kernel(NodeArgs<Real> A, NodePml<Real> P, long long g0) {
-    const long long total = (A.n_node - g0) * NFLD;
+    const long long g1 = (MULTI && A.live_node_end) ? min(A.n_node, A.live_node_end[1]) : A.n_node;
+    const long long total = max(0LL, g1 - g0) * NFLD;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
         const long long gl = t / NFLD;
@@ -458,7 +460,8 @@ __global__ void __launch_bounds__(256, 3) node_update_kernel(NodeArgs<Real> A, N
 
 template <typename Real, int NFLD, bool MULTI>
 __global__ void __launch_bounds__(256, 2) node_pml_kernel(NodeArgs<Real> A, NodePml<Real> P) {
-    const long long total = P.n_slot * NFLD;
+    const long long n1 = (MULTI && A.live_node_end) ? min(P.n_slot, A.live_node_end[0]) : P.n_slot;
+    const long long total = n1 * NFLD;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
         const long long g = t / NFLD;
@@ -487,6 +490,33 @@ __global__ void step_begin_kernel(int n_model, int* mstep, const int* nsteps, co
     mlive[m] = live ? 1 : 0;
     mstf[m] = (live && t < n_stf[m]) ? stf_all[stf_off[m] + t] : Real(0);
     mstep[m] = t + (live ? 1 : 0);
+}
+
+// Several models in one solver: after step_begin_kernel, the end of the
+// cells still stepping in each colour and of the nodes still stepping in the
+// C-PML and plain node ranges.  Cells of a colour and nodes of a range are
+// grouped by model, so everything past the largest end of a live model
+// belongs to finished models and the launches of this step stop there
+// (cells and nodes before it of finished models are still skipped one by
+// one).  cell_end [model][colour], node_end [model][2] (C-PML, plain); one
+// block, a thread per colour or range.
+static __global__ void live_bounds_kernel(int n_model, int n_colour, const int* mlive, const int* cell_end,
+                                   const int* colour_first, const long long* node_end, long long plain_first,
+                                   int* live_cell_end, long long* live_node_end) {
+    for (int c = threadIdx.x; c < n_colour + 2; c += blockDim.x) {
+        if (c < n_colour) {
+            int e = colour_first[c];
+            for (int m = 0; m < n_model; ++m)
+                if (mlive[m]) e = max(e, cell_end[m * n_colour + c]);
+            live_cell_end[c] = e;
+        } else {
+            const int r = c - n_colour;
+            long long g = r == 0 ? 0 : plain_first;
+            for (int m = 0; m < n_model; ++m)
+                if (mlive[m]) g = max(g, node_end[m * 2 + r]);
+            live_node_end[r] = g;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -847,6 +877,8 @@ struct ColShape {
 
 struct ColArgs {
     int e_begin, e_end, n_groups;
+    const int* live_end;           // [colour] end of the stepping cells (several models), or null
+    int colour;
     const uint32_t* ibool_padded;  // [cell][ib_row_words(NN)]: node words, model index
     const float* geom;             // [cell][12][NN]
     const float* ut;               // [node][NFLD][4]
@@ -875,6 +907,10 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     float* fz = fe + S::ARR;                                          // [3][GR][SP] zeta flux
     float* sD = fz + S::ARR;
 
+    // cells of this colour that still step (several models: the cells past
+    // the last one of a live model belong to finished models)
+    const int e_end = A.live_end ? min(A.e_end, A.live_end[A.colour]) : A.e_end;
+    const int n_groups = e_end > A.e_begin ? (e_end - A.e_begin + EPB - 1) / EPB : 0;
     const int tid = threadIdx.x;
     const bool lane_ok = tid < S::ACTIVE;
     const int line = lane_ok ? tid / NG2 : 0;  // (cell, wavefield) line of this thread
@@ -911,7 +947,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         for (int q = tid; q < EPB * CI; q += S::THREADS) {
             const int c = q / CI, r = q - c * CI;
             const int e = A.e_begin + grp * EPB + c;
-            if (e < A.e_end)
+            if (e < e_end)
                 cp_async16(ibase + (st * EPB + c) * S::IB_B + r * 16,
                            reinterpret_cast<const unsigned char*>(A.ibool_padded) + (size_t)e * S::IB_B + r * 16);
         }
@@ -921,14 +957,14 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         for (int q = tid; q < EPB * CG; q += S::THREADS) {
             const int c = q / CG, r = q - c * CG;
             const int e = A.e_begin + grp * EPB + c;
-            if (e < A.e_end)
+            if (e < e_end)
                 cp_async16(gbase + (st * EPB + c) * S::GEO_SLOT + r * 16,
                            reinterpret_cast<const unsigned char*>(A.geom) + (size_t)e * S::GEO_B + r * 16);
         }
     };
     // node words of this thread's line of group grp (node table in stage st)
     auto line_nodes = [&](int grp, int st, uint32_t (&w)[NG]) -> bool {
-        const bool ok = lane_ok && grp < A.n_groups && A.e_begin + grp * EPB + cl < A.e_end;
+        const bool ok = lane_ok && grp < n_groups && A.e_begin + grp * EPB + cl < e_end;
 #pragma unroll
         for (int i = 0; i < NG; ++i) w[i] = ok ? ib_of(st, cl)[i * NG2 + col] : 0u;
         return ok;
@@ -942,7 +978,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
 
     const int G = gridDim.x;
     const int grp0 = blockIdx.x;
-    if (grp0 < A.n_groups) issue_ib(grp0, 0);
+    if (grp0 < n_groups) issue_ib(grp0, 0);
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
@@ -950,8 +986,8 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     float4 pre[NG];
     bool pre_ok = line_nodes(grp0, 0, nw);
     load_vectors(nw, pre_ok, pre);
-    if (grp0 < A.n_groups) issue_geo(grp0, 0);
-    if (grp0 + G < A.n_groups) issue_ib(grp0 + G, 1);
+    if (grp0 < n_groups) issue_geo(grp0, 0);
+    if (grp0 + G < n_groups) issue_ib(grp0 + G, 1);
     cp_async_commit();
 
     const int ubase = line * SP + col;        // + c*GR*SP + i*NG2
@@ -959,7 +995,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     const int zbase = line * SP + j * NG;        // + s     (zeta line: i*NG2 + j*NG + s)
 
     int it = 0;
-    for (int grp = grp0; grp < A.n_groups; grp += G, ++it) {
+    for (int grp = grp0; grp < n_groups; grp += G, ++it) {
         const int e = A.e_begin + grp * EPB + cl;
         const int mdl = pre_ok ? (int)ib_of(it % 3, cl)[NN] : 0;
         const bool act = pre_ok && s_live[mdl];
@@ -980,8 +1016,8 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         cp_async_wait_all();
         __syncthreads();  // displacement of this group, its geometry, the next node table
         const int nx = grp + G;
-        if (nx < A.n_groups) issue_geo(nx, (it + 1) & 1);
-        if (nx + G < A.n_groups) issue_ib(nx + G, (it + 2) % 3);
+        if (nx < n_groups) issue_geo(nx, (it + 1) & 1);
+        if (nx + G < n_groups) issue_ib(nx + G, (it + 2) % 3);
         cp_async_commit();
         // old force vectors of the nodes this colour does not touch first:
         // start their DRAM reads into L2 now, so the loads issued after the

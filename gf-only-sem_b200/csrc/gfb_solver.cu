@@ -212,6 +212,13 @@ struct gfb_solver {
     std::vector<int> model_nsteps;
     gfb::ModelConst* d_mc = nullptr;
     uint8_t* d_node_model = nullptr;   // [node] (several models only)
+    // several models: per model the end of its cells in each colour and of
+    // its nodes in the C-PML and plain ranges; the bounds of this step
+    int* d_cell_end = nullptr;          // [model][colour]
+    int* d_colour_first = nullptr;      // [colour]
+    long long* d_node_end = nullptr;    // [model][2]
+    int* d_live_cell_end = nullptr;     // [colour]
+    long long* d_live_node_end = nullptr;  // [2]
     int *d_mlive = nullptr, *d_mstep = nullptr, *d_nsteps = nullptr, *d_nstf = nullptr;
     long long* d_stf_off = nullptr;
     void *d_mstf = nullptr, *d_stf_all = nullptr;
@@ -418,6 +425,7 @@ void node_args(const gfb_solver* s, gfb::NodeArgs<Real>& A, gfb::NodePml<Real>& 
     A.node_model = s->d_node_model;
     A.mc = s->d_mc;
     A.mlive = s->d_mlive;
+    A.live_node_end = s->d_live_node_end;  // null with one model
     P = gfb::NodePml<Real>{};
     if (s->node_pml) {
         P.coef = static_cast<const Real*>(s->npml_coef);
@@ -487,6 +495,8 @@ gfb_status launch_col_e(gfb_solver* s, int c) {
     if (A.e_end <= A.e_begin) return GFB_OK;
     const int n = A.e_end - A.e_begin;
     A.n_groups = (n + S::EPB - 1) / S::EPB;
+    A.live_end = s->d_live_cell_end;  // null with one model
+    A.colour = c;
     A.ibool_padded = s->ibool_padded;
     A.geom = static_cast<const float*>(s->geom);
     A.ut = static_cast<const float*>(s->ut);
@@ -1250,6 +1260,39 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
                 for (int g = models[k].node_begin; g < models[k].node_end; ++g) nm[dev_node(g)] = (uint8_t)k;
             if ((st = s->alloc(&s->d_node_model, nm.size()))) return st;
             if ((st = h2d(s, s->d_node_model, nm.data(), nm.size()))) return st;
+            // ends of each model's cells per colour and nodes per range
+            const int nc = (int)s->colour_begin.size() - 1;
+            const long long g0 = s->node_pml ? s->n_pml_node : 0;
+            std::vector<int> cell_end((size_t)n_model * nc), first(nc), live_cell(nc);
+            for (int k = 0; k < n_model; ++k)
+                for (int c = 0; c < nc; ++c) cell_end[(size_t)k * nc + c] = s->colour_begin[c];
+            for (int c = 0; c < nc; ++c) {
+                first[c] = s->colour_begin[c];
+                live_cell[c] = s->colour_begin[c + 1];
+                for (int ed = s->colour_begin[c]; ed < s->colour_begin[c + 1]; ++ed) {
+                    int mi = 0;
+                    while (perm[ed] >= models[mi].cell_end) ++mi;
+                    cell_end[(size_t)mi * nc + c] = ed + 1;
+                }
+            }
+            std::vector<long long> node_end((size_t)n_model * 2), live_node{g0, (long long)s->n_node};
+            for (int k = 0; k < n_model; ++k) {
+                node_end[(size_t)k * 2] = 0;
+                node_end[(size_t)k * 2 + 1] = g0;
+            }
+            for (long long d = 0; d < s->n_node; ++d) {
+                long long& e = node_end[(size_t)nm[d] * 2 + (d < g0 ? 0 : 1)];
+                e = std::max(e, d + 1);
+            }
+            auto put = [&](auto** dst, const auto& h) -> gfb_status {
+                gfb_status r;
+                if ((r = s->alloc(dst, h.size()))) return r;
+                return h2d(s, *dst, h.data(), h.size() * sizeof(h[0]));
+            };
+            if ((st = put(&s->d_cell_end, cell_end)) || (st = put(&s->d_colour_first, first)) ||
+                (st = put(&s->d_live_cell_end, live_cell)) || (st = put(&s->d_node_end, node_end)) ||
+                (st = put(&s->d_live_node_end, live_node)))
+                return st;
         }
     }
     if (s->node_pml) {
@@ -1319,6 +1362,15 @@ gfb_status launch_step_begin_t(gfb_solver* s) {
         static_cast<Real*>(s->d_mstf), s->d_mlive);
     CU(cudaGetLastError());
     s->launches++;
+    if (s->d_live_cell_end) {
+        const int nc = (int)s->colour_begin.size() - 1;
+        gfb::live_bounds_kernel<<<1, 128, 0, s->stream>>>(s->n_model, nc, s->d_mlive, s->d_cell_end,
+                                                          s->d_colour_first, s->d_node_end,
+                                                          s->node_pml ? (long long)s->n_pml_node : 0LL,
+                                                          s->d_live_cell_end, s->d_live_node_end);
+        CU(cudaGetLastError());
+        s->launches++;
+    }
     return GFB_OK;
 }
 
