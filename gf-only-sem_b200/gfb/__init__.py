@@ -532,20 +532,32 @@ class BatchSolver(Solver):
     ``probs`` are per-model problem dicts (gfb.mesh.build_problem layout);
     ``n_steps`` the steps each model takes (default: its "nsteps").  The
     models share ngll, snapshot stride, precision and wavefield directions.
+
+    The models are placed in the solver in decreasing order of their step
+    counts, so the ones that have finished are always the last cells of
+    each colour and the last nodes: each step's launches stop before them.
+    Model indices in this class's methods are the caller's.
     """
 
     def __init__(self, probs: Sequence[dict], dirs: Sequence[int] = (0,), precision: int = FP64,
                  device: int = 0, record_slots: int = 4, flags: int = 0, n_steps: Optional[Sequence[int]] = None):
-        merged, models, layout = merge_problems(probs, n_steps)
+        steps = [int(n) for n in (n_steps if n_steps is not None else [p["nsteps"] for p in probs])]
+        self.placement = sorted(range(len(probs)), key=lambda k: -steps[k])  # position -> caller index
+        self.position = [0] * len(probs)  # caller index -> position
+        for pos, k in enumerate(self.placement):
+            self.position[k] = pos
+        merged, models, layout = merge_problems([probs[k] for k in self.placement],
+                                                [steps[k] for k in self.placement])
         super().__init__(merged, dirs=dirs, precision=precision, device=device, record_slots=record_slots,
                          flags=flags, models=models)
-        self.models = models
-        self.layout = layout
+        self.models = models  # in placement order
+        self.layout = layout  # in placement order
         self.n_model = len(models)
 
     def model_state(self, k: int, field: int = 0):
         u, v, a = self.state(field)
-        a0, a1 = self.layout["node_off"][k], self.layout["node_off"][k + 1]
+        pos = self.position[k]
+        a0, a1 = self.layout["node_off"][pos], self.layout["node_off"][pos + 1]
         return u[a0:a1], v[a0:a1], a[a0:a1]
 
     def drain_models(self):
@@ -555,11 +567,12 @@ class BatchSolver(Solver):
         snaps = self.drain()
         out = []
         for k in range(self.n_model):
-            r0, r1 = self.layout["rec_off"][k], self.layout["rec_off"][k + 1]
+            pos = self.position[k]
+            r0, r1 = self.layout["rec_off"][pos], self.layout["rec_off"][pos + 1]
             per = {}
             for f, d in snaps.items():
                 steps = np.asarray(d["steps"])
-                keep = steps < self.models[k]["n_steps"]
+                keep = steps < self.models[pos]["n_steps"]
                 per[f] = {"steps": steps[keep]}
                 for name in ("strain", "u", "v", "a"):
                     x = np.asarray(d[name])
