@@ -140,6 +140,70 @@ void parallel_compact(long long n, Keep&& keep, Value&& value, std::vector<int>&
     }, 1);
 }
 
+// The points of the mesh grouped by the thread that owns their node.
+// Owner t holds the nodes [bound[t], bound[t+1]) and the points q that list
+// one of them, in increasing q: q[off[t] .. off[t+1]).  Built once by a
+// parallel partition of the points; a pass that must visit each node's
+// points in mesh order (sums in the reference's order) then reads only its
+// own points instead of scanning every point per thread.
+struct NodeBuckets {
+    int n_owner = 1;
+    long long n_node = 0;
+    std::vector<long long> bound;  // [n_owner + 1]
+    std::vector<size_t> off;       // [n_owner + 1]
+    std::vector<long long> q;      // [points]
+    int owner(long long g) const {
+        int t = (int)(g * n_owner / std::max(1LL, n_node));
+        while (t + 1 < n_owner && bound[t + 1] <= g) ++t;
+        while (t > 0 && bound[t] > g) --t;
+        return t;
+    }
+    // fn(t, g0, g1, points, count) on one thread per owner
+    template <typename F>
+    void for_each_owner(F&& fn) const {
+        std::vector<std::thread> th;
+        for (int t = 0; t < n_owner; ++t)
+            th.emplace_back([&, t] { fn(t, bound[t], bound[t + 1], q.data() + off[t], off[t + 1] - off[t]); });
+        for (auto& x : th) x.join();
+    }
+};
+
+NodeBuckets bucket_points(const int* ibool, long long P, long long n_node) {
+    NodeBuckets b;
+    const long long hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    b.n_owner = (int)std::max(1LL, std::min(hw, n_node / (1LL << 18)));
+    b.n_node = n_node;
+    const int T = b.n_owner;
+    b.bound.resize(T + 1);
+    for (int t = 0; t <= T; ++t) b.bound[t] = n_node * t / T;
+    const long long n_chunk = std::max(1LL, std::min<long long>(4 * hw, P / 65536));
+    auto cb = [&](long long c) { return P * c / n_chunk; };
+    std::vector<size_t> pos((size_t)n_chunk * T, 0);
+    parallel_for(n_chunk, [&](long long c0, long long c1) {
+        for (long long c = c0; c < c1; ++c)
+            for (long long q = cb(c); q < cb(c + 1); ++q) pos[(size_t)c * T + b.owner(ibool[q])]++;
+    }, 1);
+    b.off.assign(T + 1, 0);
+    size_t run = 0;
+    for (int t = 0; t < T; ++t) {
+        b.off[t] = run;
+        for (long long c = 0; c < n_chunk; ++c) {
+            const size_t k = pos[(size_t)c * T + t];
+            pos[(size_t)c * T + t] = run;
+            run += k;
+        }
+    }
+    b.off[T] = run;
+    b.q.resize(run);
+    parallel_for(n_chunk, [&](long long c0, long long c1) {
+        for (long long c = c0; c < c1; ++c) {
+            size_t* pc = pos.data() + (size_t)c * T;
+            for (long long q = cb(c); q < cb(c + 1); ++q) b.q[pc[b.owner(ibool[q])]++] = q;
+        }
+    }, 1);
+    return b;
+}
+
 struct DevBuf {
     void* p = nullptr;
     ~DevBuf() {
@@ -832,70 +896,62 @@ gfb_status spill(gfb_solver* s, Snapshot& snap) {
 // Returns false (per-cell form) if two cells disagree on an axis's
 // coefficients at a shared node (beyond 1e-6 relative).  slot[g] numbers the C-PML nodes in
 // increasing node order; coef is [slot][14].
-bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w, std::vector<int>& slot,
-                   std::vector<double>& coef) {
+bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w, const NodeBuckets& nb,
+                   std::vector<int>& slot, std::vector<double>& coef) {
     const int ng = s->ng, nn = s->nn;
     auto live = [&](long long q) {
+        if (m->pml_region[q / nn] == 0) return false;
         const double* A = m->pml_coef_abar + q * 5;
         return A[0] != 0.0 || A[1] != 0.0 || A[2] != 0.0 || A[3] != 0.0 || A[4] != 0.0;
     };
-    std::vector<int> pcell;
-    for (long long e = 0; e < s->n_cell; ++e)
-        if (m->pml_region[e] != 0) pcell.push_back((int)e);
-    // each thread owns a range of nodes and visits the C-PML cells in mesh
-    // order, so every node accumulates in the same order as one pass would
+    // each thread goes through the points of its own nodes in mesh order,
+    // so every node accumulates in the same order as one pass would
     slot.assign(s->n_node, -1);
-    parallel_for(s->n_node, [&](long long g0, long long g1) {
-        for (int e : pcell)
-            for (int p = 0; p < nn; ++p) {
-                const long long q = (long long)e * nn + p;
-                const int g = m->ibool[q];
-                if (g >= g0 && g < g1 && live(q)) slot[g] = 0;
-            }
-    }, 1 << 18);
+    nb.for_each_owner([&](int, long long, long long, const long long* qs, size_t nq) {
+        for (size_t k = 0; k < nq; ++k)
+            if (live(qs[k])) slot[m->ibool[qs[k]]] = 0;
+    });
     int n = 0;
     for (int g = 0; g < s->n_node; ++g)
         if (slot[g] >= 0) slot[g] = n++;
     coef.assign((size_t)n * 14, 0.0);
     std::vector<unsigned char> have(n, 0);
     std::atomic<bool> agree(true);
-    parallel_for(s->n_node, [&](long long g0, long long g1) {
-        for (int e : pcell) {
-            for (int p = 0; p < nn; ++p) {
-                const long long q = (long long)e * nn + p;
-                const int g = m->ibool[q];
-                if (g < g0 || g >= g1 || !live(q)) continue;
-                const double* A = m->pml_coef_abar + q * 5;
-                const int sl = slot[g];
-                double* c = &coef[(size_t)sl * 14];
-                const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
-                const double wgll = w[ni] * w[nj] * w[nk];
-                const double rho = m->density[q];
-                const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
-                for (int k = 0; k < 5; ++k) c[k] += scale * A[k];
-                const double* al = m->pml_coef_alpha + q * 9;
-                for (int ax = 0; ax < 3; ++ax) {
-                    if (A[2 + ax] == 0.0) continue;
-                    if (!(have[sl] & (1u << ax))) {
-                        for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
-                        have[sl] |= (unsigned char)(1u << ax);
-                    } else {
-                        for (int t = 0; t < 3; ++t) {
-                            const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
-                            // the cells' coefficients at a node come from the same position
-                            // through different cell maps: equal up to rounding (seen up to
-                            // ~1e-9 relative on deformed meshes); different profiles differ
-                            // at O(1)
-                            if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) {
-                                agree.store(false);
-                                return;
-                            }
+    nb.for_each_owner([&](int, long long, long long, const long long* qs, size_t nq) {
+        for (size_t k = 0; k < nq; ++k) {
+            const long long q = qs[k];
+            if (!live(q)) continue;
+            const int p = (int)(q % nn);
+            const double* A = m->pml_coef_abar + q * 5;
+            const int sl = slot[m->ibool[q]];
+            double* c = &coef[(size_t)sl * 14];
+            const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
+            const double wgll = w[ni] * w[nj] * w[nk];
+            const double rho = m->density[q];
+            const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
+            for (int kk = 0; kk < 5; ++kk) c[kk] += scale * A[kk];
+            const double* al = m->pml_coef_alpha + q * 9;
+            for (int ax = 0; ax < 3; ++ax) {
+                if (A[2 + ax] == 0.0) continue;
+                if (!(have[sl] & (1u << ax))) {
+                    for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
+                    have[sl] |= (unsigned char)(1u << ax);
+                } else {
+                    for (int t = 0; t < 3; ++t) {
+                        const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
+                        // the cells' coefficients at a node come from the same position
+                        // through different cell maps: equal up to rounding (seen up to
+                        // ~1e-9 relative on deformed meshes); different profiles differ
+                        // at O(1)
+                        if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) {
+                            agree.store(false);
+                            return;
                         }
                     }
                 }
             }
         }
-    }, 1 << 18);
+    });
     return agree.load();
 }
 
@@ -927,7 +983,8 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
                         const gfb_model* models, const std::vector<int>& perm, const std::vector<int>& inv_perm,
                         const std::vector<uint32_t>& ibool_dev, const std::vector<double>& node_mass,
                         const std::vector<double>& node_damp, const std::vector<long long>& first_q,
-                        const std::vector<double>& w, const std::vector<double>& D, StageClock& clk) {
+                        std::vector<uint8_t>& first_flag, const NodeBuckets& nb, const std::vector<double>& w,
+                        const std::vector<double>& D, StageClock& clk) {
     const int ng = s->ng, nn = s->nn;
     const long long n_cell = s->n_cell;
     gfb_status st;
@@ -974,20 +1031,25 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     std::vector<int> pslot;
     std::vector<double> pcoef;
     const bool node_form = s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML) &&
-                           plan_node_pml(s, m, w, pslot, pcoef);
+                           plan_node_pml(s, m, w, nb, pslot, pcoef);
     clk.mark("C-PML node plan");
     {
-        // a point q is its node's first touch when first_q[node] == q
+        // first_flag[q]: 1 if q is its node's first touch, 2 if that node is
+        // also a node-form C-PML node
         s->node_perm.clear();
         s->node_inv.clear();
         s->node_perm.reserve(s->n_node);
         const long long P = n_cell * nn;
+        if (node_form)
+            parallel_for(s->n_node, [&](long long g0, long long g1) {
+                for (long long g = g0; g < g1; ++g)
+                    if (pslot[g] >= 0) first_flag[first_q[g]] = 2;
+            });
         auto node_of = [&](long long q) { return m->ibool[q]; };
-        for (int pass = node_form ? 0 : 1; pass < 2; ++pass)
-            parallel_compact(P, [&](long long q) {
-                const int g = m->ibool[q];
-                return first_q[g] == q && (pass == 1 ? (!node_form || pslot[g] < 0) : pslot[g] >= 0);
-            }, node_of, s->node_perm);
+        for (int pass = node_form ? 0 : 1; pass < 2; ++pass) {
+            const uint8_t want = pass == 0 ? 2 : 1;
+            parallel_compact(P, [&](long long q) { return first_flag[q] == want; }, node_of, s->node_perm);
+        }
         parallel_compact(s->n_node, [&](long long g) { return first_q[g] < 0; },  // nodes no cell uses
                          [](long long g) { return (int)g; }, s->node_perm);
         std::atomic<bool> ident(true);
@@ -1610,17 +1672,23 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     // so every node sums (and assigns) in the reference's order
     // The same pass records each node's first touch (the first point in
     // mesh order that lists it), from which the device numbering follows.
+    const NodeBuckets nb = bucket_points(m->ibool, P, m->n_node);
+    clk.mark("point buckets");
     std::vector<double> node_mass(m->n_node, 0.0), node_damp(m->n_node, 0.0);
     std::vector<long long> first_q(m->n_node, -1);
-    parallel_for(m->n_node, [&](long long g0, long long g1) {
-        for (long long q = 0; q < P; ++q) {
+    std::vector<uint8_t> first_flag((size_t)P, 0);  // 1: the point is its node's first touch
+    nb.for_each_owner([&](int, long long, long long, const long long* qs, size_t nq) {
+        for (size_t k = 0; k < nq; ++k) {
+            const long long q = qs[k];
             const int g = m->ibool[q];
-            if (g < g0 || g >= g1) continue;
             node_mass[g] += m->mass[q];
             node_damp[g] = m->damping ? m->damping[q] : 0.0;
-            if (first_q[g] < 0) first_q[g] = q;
+            if (first_q[g] < 0) {
+                first_q[g] = q;
+                first_flag[q] = 1;
+            }
         }
-    }, 1 << 18);
+    });
     clk.mark("lumped mass");
     s->has_damping = false;
     if (!s->has_cpml && m->damping)
@@ -1680,11 +1748,11 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     if (s->prec == GFB_FP64) {
         if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<double>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                  first_q, w, D, clk);
+                                  first_q, first_flag, nb, w, D, clk);
     } else {
         if ((st = dispatch<float, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<float>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                 first_q, w, D, clk);
+                                 first_q, first_flag, nb, w, D, clk);
     }
     if (st) return st;
     CU(cudaStreamSynchronize(s->stream));
