@@ -962,10 +962,16 @@ template <typename Real>
 gfb_status upload_node_pml(gfb_solver* s, const std::vector<double>& coef) {
     gfb_status st;
     const int n = (int)(coef.size() / 14);
-    std::vector<Real> cf(coef.size());
-    for (size_t i = 0; i < coef.size(); ++i) cf[i] = (Real)coef[i];
-    if (cf.empty()) cf.push_back(Real(0));
-    if ((st = upload(s, &s->npml_coef, cf))) return st;
+    Real* dc = nullptr;
+    if ((st = s->alloc(&dc, (size_t)std::max(n, 1) * 14))) return st;
+    st = staged_upload(s, dc, 14 * sizeof(Real), n, [&](long long i0, long long i1, unsigned char* out) {
+        Real* o = reinterpret_cast<Real*>(out);
+        parallel_for((i1 - i0) * 14, [&](long long a0, long long a1) {
+            for (long long i = a0; i < a1; ++i) o[i] = (Real)coef[(size_t)i0 * 14 + i];
+        });
+    });
+    if (st) return st;
+    s->npml_coef = dc;
     Real *mem = nullptr, *prev = nullptr;
     if ((st = s->alloc(&mem, (size_t)std::max(n, 1) * s->F * 3))) return st;
     if ((st = s->alloc(&prev, (size_t)std::max(n, 1) * s->F))) return st;
@@ -1181,23 +1187,38 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     CU(cudaMemset(ut, 0, nP * sizeof(Real)));
     CU(cudaMemset(force, 0, nP * sizeof(Real)));
     clk.mark("state arrays");
-    const std::vector<double> mass_d = permuted(node_mass);
+    // lumped mass, 1/m (FP32 path; 0 marks m <= 0) and damping in device
+    // order, gathered by the host threads straight into the pinned chunks
+    auto gathered = [&](void* dst, size_t es, auto value) -> gfb_status {
+        return staged_upload(s, dst, es, s->n_node, [&](long long i0, long long i1, unsigned char* out) {
+            parallel_for(i1 - i0, [&](long long a0, long long a1) {
+                for (long long i = a0; i < a1; ++i) {
+                    const long long d = i0 + i;
+                    value(s->node_perm.empty() ? d : (long long)s->node_perm[d], out + (size_t)i * es);
+                }
+            }, 65536);
+        });
+    };
     {
         double* d = nullptr;
-        if ((st = s->alloc(&d, mass_d.size()))) return st;
-        if ((st = h2d(s, d, mass_d.data(), mass_d.size() * 8))) return st;
+        if ((st = s->alloc(&d, (size_t)s->n_node))) return st;
+        if ((st = gathered(d, 8, [&](long long g, unsigned char* o) { std::memcpy(o, &node_mass[g], 8); }))) return st;
         s->mass = d;
     }
     if (s->prec == GFB_FP32) {
-        std::vector<Real> im(mass_d.size());
-        for (size_t g = 0; g < im.size(); ++g) im[g] = mass_d[g] > 0.0 ? (Real)(1.0 / mass_d[g]) : Real(0);
-        if ((st = upload(s, &s->inv_mass, im))) return st;
+        Real* d = nullptr;
+        if ((st = s->alloc(&d, (size_t)s->n_node))) return st;
+        st = gathered(d, sizeof(Real), [&](long long g, unsigned char* o) {
+            const Real im = node_mass[g] > 0.0 ? (Real)(1.0 / node_mass[g]) : Real(0);
+            std::memcpy(o, &im, sizeof(Real));
+        });
+        if (st) return st;
+        s->inv_mass = d;
     }
     if (s->has_damping) {
-        const std::vector<double> damp_d = permuted(node_damp);
         double* d = nullptr;
-        if ((st = s->alloc(&d, damp_d.size()))) return st;
-        if ((st = h2d(s, d, damp_d.data(), damp_d.size() * 8))) return st;
+        if ((st = s->alloc(&d, (size_t)s->n_node))) return st;
+        if ((st = gathered(d, 8, [&](long long g, unsigned char* o) { std::memcpy(o, &node_damp[g], 8); }))) return st;
         s->damping = d;
     }
     clk.mark("mass and damping");
