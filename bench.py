@@ -693,7 +693,7 @@ def run_gfb(args):
     s2 = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8, flags=flags)
     t_create = time.perf_counter() - t0
     up = s2.info()["upload_bytes"]
-    rec = s2.run(args.steps)
+    rec = s2.run(args.steps, dtype=np.float32 if args.record_f32 else np.float64)
     s2.synchronize()
     s2.close()
     e2e_t = time.perf_counter() - t0
@@ -736,7 +736,7 @@ def run_gfb(args):
                 "d2h_bytes_per_step": rec_bytes / args.steps,
                 "create_s": t_create, "total_s": e2e_t,
                 "note": "gfb_create from host arrays + K steps with every snapshot read into host arrays "
-                        "(Solver.run) + destroy"},
+                        "(Solver.run, in the recorded precision) + destroy"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

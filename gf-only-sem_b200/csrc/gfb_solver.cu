@@ -847,19 +847,19 @@ size_t snapshot_bytes(const gfb_solver* s) { return snapshot_values(s) * (s->rec
 // the caller's arrays: output point q takes the 15 values at
 // raw + src_index(q) * 15 (float or double as recorded).  Threads split the
 // points; a NULL array is skipped.
-template <typename Index>
-void unpack_points(const gfb_solver* s, const void* raw, long long n_out, Index src_index, double* strain, double* u,
-                   double* v, double* a) {
+template <typename Index, typename Out>
+void unpack_points(const gfb_solver* s, const void* raw, long long n_out, Index src_index, Out* strain, Out* u,
+                   Out* v, Out* a) {
     auto run = [&](auto* src) {
         parallel_for(n_out, [&](long long q0, long long q1) {
             for (long long q = q0; q < q1; ++q) {
                 const auto* o = src + (size_t)src_index(q) * 15;
                 if (strain)
-                    for (int c = 0; c < 6; ++c) strain[q * 6 + c] = (double)o[c];
+                    for (int c = 0; c < 6; ++c) strain[q * 6 + c] = (Out)o[c];
                 for (int c = 0; c < 3; ++c) {
-                    if (u) u[q * 3 + c] = (double)o[6 + c];
-                    if (v) v[q * 3 + c] = (double)o[9 + c];
-                    if (a) a[q * 3 + c] = (double)o[12 + c];
+                    if (u) u[q * 3 + c] = (Out)o[6 + c];
+                    if (v) v[q * 3 + c] = (Out)o[9 + c];
+                    if (a) a[q * 3 + c] = (Out)o[12 + c];
                 }
             }
         }, 16384);
@@ -2141,8 +2141,14 @@ gfb_status gfb_records_pending(gfb_solver* s, int32_t* n) {
     return GFB_OK;
 }
 
-gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* strain, double* u,
-                           double* v, double* a, int32_t release) {
+}  // extern "C"
+
+namespace {
+
+// gfb_read_record into double or float buffers.
+template <typename Out>
+gfb_status read_record_t(gfb_solver* s, int32_t field, int32_t* step, Out* strain, Out* u, Out* v, Out* a,
+                         int32_t release) {
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (field < 0 || field >= s->nfld) return fail(GFB_ERR_INVALID, "field %d out of range", field);
     CU(cudaSetDevice(s->device));
@@ -2183,6 +2189,20 @@ gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* 
     }
     s->rec_cv.notify_all();
     return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+gfb_status gfb_read_record(gfb_solver* s, int32_t field, int32_t* step, double* strain, double* u,
+                           double* v, double* a, int32_t release) {
+    return read_record_t(s, field, step, strain, u, v, a, release);
+}
+
+gfb_status gfb_read_record_f32(gfb_solver* s, int32_t field, int32_t* step, float* strain, float* u, float* v,
+                               float* a, int32_t release) {
+    return read_record_t(s, field, step, strain, u, v, a, release);
 }
 
 gfb_status gfb_rec_nodes(gfb_solver* s, int32_t* n_node, int64_t* node_ids) {

@@ -151,6 +151,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.gfb_set_state.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp, _dp]
     lib.gfb_records_pending.argtypes = [C.c_void_p, _ip]
     lib.gfb_read_record.argtypes = [C.c_void_p, C.c_int32, _ip, _dp, _dp, _dp, _dp, C.c_int32]
+    _fp = C.POINTER(C.c_float)
+    lib.gfb_read_record_f32.argtypes = [C.c_void_p, C.c_int32, _ip, _fp, _fp, _fp, _fp, C.c_int32]
     lib.gfb_element_residual.argtypes = [C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int32, _dp, _dp, C.c_int32, C.c_int32]
     lib.gfb_run_forward.argtypes = [C.c_char_p, C.c_int32, C.c_int32]
     lib.gfb_run_forward.restype = C.c_int32
@@ -159,7 +161,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "gfb_get_state", "gfb_set_state", "gfb_records_pending", "gfb_read_record",
         "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
         "gfb_create_batch", "gfb_checkpoint_size", "gfb_checkpoint_save", "gfb_checkpoint_load",
-        "gfb_rec_nodes", "gfb_read_green",
+        "gfb_rec_nodes", "gfb_read_green", "gfb_read_record_f32",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -335,31 +337,39 @@ class Solver:
         _check(self.lib.gfb_records_pending(self.h, C.byref(n)))
         return n.value
 
-    def _record_arrays(self, n: Optional[int] = None):
+    def _record_arrays(self, n: Optional[int] = None, dtype=np.float64):
         lead = () if n is None else (n,)
-        out = {"strain": np.empty(lead + (self.n_rec, self.nn, 6))}
+        out = {"strain": np.empty(lead + (self.n_rec, self.nn, 6), dtype=dtype)}
         for k in ("u", "v", "a"):
-            out[k] = np.empty(lead + (self.n_rec, self.nn, 3))
+            out[k] = np.empty(lead + (self.n_rec, self.nn, 3), dtype=dtype)
         return out
 
-    def read_record(self, field: int = 0, release: bool = False, out: Optional[dict] = None):
+    def read_record(self, field: int = 0, release: bool = False, out: Optional[dict] = None, dtype=np.float64):
         """Oldest unread snapshot of one field: strain [cell][point][6],
-        u, v, a [cell][point][3] over the recording cells.  ``out`` gives
-        C-contiguous float64 arrays of those shapes to fill instead of new
-        ones (a missing key is not read)."""
+        u, v, a [cell][point][3] over the recording cells, float64 or
+        float32 (``dtype``; float32 is what the reference writes with
+        snapshot_precision "float32").  ``out`` gives C-contiguous arrays of
+        those shapes and one of the two types to fill instead of new ones (a
+        missing key is not read)."""
         step = C.c_int32()
         if out is None:
-            out = self._record_arrays()
-        arrs = {}
+            out = self._record_arrays(dtype=dtype)
+        arrs, types = {}, set()
         for k, last in (("strain", 6), ("u", 3), ("v", 3), ("a", 3)):
             x = out.get(k)
-            if x is not None and (x.dtype != np.float64 or not x.flags.c_contiguous
-                                  or x.shape != (self.n_rec, self.nn, last)):
-                raise ValueError(f"out[{k!r}] must be C-contiguous float64 of shape {(self.n_rec, self.nn, last)}")
+            if x is not None:
+                if (x.dtype not in (np.float64, np.float32) or not x.flags.c_contiguous
+                        or x.shape != (self.n_rec, self.nn, last)):
+                    raise ValueError(f"out[{k!r}] must be C-contiguous float64 or float32 of shape "
+                                     f"{(self.n_rec, self.nn, last)}")
+                types.add(x.dtype)
             arrs[k] = x
-        _check(self.lib.gfb_read_record(self.h, field, C.byref(step),
-                                        *[_ptr(arrs[k], C.c_double) for k in ("strain", "u", "v", "a")],
-                                        1 if release else 0))
+        if len(types) > 1:
+            raise ValueError("out arrays must share one dtype")
+        f32 = types == {np.dtype(np.float32)}
+        fn, ct = (self.lib.gfb_read_record_f32, C.c_float) if f32 else (self.lib.gfb_read_record, C.c_double)
+        _check(fn(self.h, field, C.byref(step), *[_ptr(arrs[k], ct) for k in ("strain", "u", "v", "a")],
+                  1 if release else 0))
         return {"step": step.value, **arrs}
 
     def rec_nodes(self) -> np.ndarray:
@@ -382,14 +392,14 @@ class Solver:
                                        _ptr(v, C.c_double), _ptr(a, C.c_double), 1 if release else 0))
         return {"step": step.value, "strain": strain, "u": u, "v": v, "a": a}
 
-    def _read_snapshots(self, n: int, wait=None):
+    def _read_snapshots(self, n: int, wait=None, dtype=np.float64):
         """n snapshots, every field, read into arrays allocated once:
         {field: {"steps": [n], "strain": [n][cell][point][6], "u"/"v"/"a":
         [n][cell][point][3]}}.  ``wait()`` is called while none is pending
         (returns False to give up)."""
         out = {}
         for f in range(self.n_field):
-            out[f] = {"steps": np.zeros(n, dtype=np.int64), **self._record_arrays(n)}
+            out[f] = {"steps": np.zeros(n, dtype=np.int64), **self._record_arrays(n, dtype)}
         for i in range(n):
             while wait is not None and self.pending() == 0:
                 if not wait():
@@ -399,11 +409,11 @@ class Solver:
                 out[f]["steps"][i] = r["step"]
         return out
 
-    def drain(self):
+    def drain(self, dtype=np.float64):
         """All pending snapshots as {field: dict of stacked arrays}."""
-        return self._read_snapshots(self.pending())
+        return self._read_snapshots(self.pending(), dtype=dtype)
 
-    def run(self, n_steps: int):
+    def run(self, n_steps: int, dtype=np.float64):
         """Advance n_steps and return every snapshot pending before them or
         recorded by them (as ``drain``), read out by a second thread while the
         steps run, as the reference's time loop writes each snapshot when it
@@ -425,7 +435,7 @@ class Solver:
 
         def reader():
             try:
-                box["out"] = self._read_snapshots(n, wait)
+                box["out"] = self._read_snapshots(n, wait, dtype)
             except BaseException as e:  # re-raised in the caller's thread
                 box["err"] = e
 

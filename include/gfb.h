@@ -91,7 +91,7 @@ typedef struct gfb_config {
 #define GFB_FLAG_CELL_PML 1
 /* Store snapshots as float on the device and in the pinned host ring (the
  * reference's snapshot_precision = "float32", record.cpp:91-98, 132-139);
- * gfb_read_record still returns doubles. */
+ * gfb_read_record still returns doubles, gfb_read_record_f32 floats. */
 #define GFB_FLAG_RECORD_F32 2
 /* Update each node in the epilogue of the element kernel of the highest
  * colour touching it instead of in a separate node pass (same results).
@@ -298,6 +298,13 @@ gfb_status gfb_records_pending(gfb_solver* solver, int32_t* n);
  */
 gfb_status gfb_read_record(gfb_solver* solver, int32_t field, int32_t* step, double* strain,
                            double* u, double* v, double* a, int32_t release);
+
+/* The same into float32 buffers: the record datasets as RecordWriter writes
+ * them with snapshot_precision = "float32" (record.cpp:91-98).  Values
+ * recorded in float (GFB_FLAG_RECORD_F32) come out unchanged; values
+ * recorded in double are rounded. */
+gfb_status gfb_read_record_f32(gfb_solver* solver, int32_t field, int32_t* step, float* strain, float* u,
+                               float* v, float* a, int32_t release);
 
 /*
  * Element internal force for n_elem independent elements, host arrays in

@@ -61,9 +61,32 @@ def test_read_record_into_caller_arrays(prob):
     assert r["u"] is u and r["strain"] is None
     np.testing.assert_array_equal(u, ref[0]["u"][0])
     with pytest.raises(ValueError):
-        s2.read_record(0, out={"v": np.zeros((s2.n_rec, s2.nn, 3), dtype=np.float32)})
+        s2.read_record(0, out={"v": np.zeros((s2.n_rec, s2.nn, 3), dtype=np.int32)})
+    # float32 read-out (gfb_read_record_f32) of this double record: rounded
+    # to float32 as numpy rounds
+    r = s2.read_record(0, dtype=np.float32)
+    assert r["u"].dtype == np.float32
+    for k in ("strain", "u", "v", "a"):
+        np.testing.assert_array_equal(r[k], ref[0][k][1].astype(np.float32))
     s.close()
     s2.close()
+
+
+def test_run_float32_equals_float64_read(prob):
+    """Solver.run with float32 arrays reads the same float records as the
+    float64 read-out, and a double record rounded to float32."""
+    for flags in (gfb.FLAG_RECORD_F32, 0):
+        a = gfb.Solver(prob, dirs=[0, 2], precision=gfb.FP32, record_slots=3, flags=flags)
+        ref = a.run(40)
+        b = gfb.Solver(prob, dirs=[0, 2], precision=gfb.FP32, record_slots=3, flags=flags)
+        got = b.run(40, dtype=np.float32)
+        for f in range(2):
+            np.testing.assert_array_equal(got[f]["steps"], ref[f]["steps"])
+            for k in ("strain", "u", "v", "a"):
+                assert got[f][k].dtype == np.float32
+                np.testing.assert_array_equal(got[f][k], ref[f][k].astype(np.float32))
+        a.close()
+        b.close()
 
 
 def test_mesh_check_reports_first_offending_entry(prob):
