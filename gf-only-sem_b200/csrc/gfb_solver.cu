@@ -1090,14 +1090,6 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     }
     clk.mark("node numbering");
     auto dev_node = [&](long long g) -> long long { return s->node_inv.empty() ? g : s->node_inv[g]; };
-    auto permuted = [&](const std::vector<double>& h) {
-        if (s->node_perm.empty()) return h;
-        std::vector<double> o(h.size());
-        parallel_for((long long)o.size(), [&](long long d0, long long d1) {
-            for (long long d = d0; d < d1; ++d) o[d] = h[s->node_perm[d]];
-        });
-        return o;
-    };
     // ibool in device node numbers, and the rows of the pipelined kernels:
     // node words, then the cell's model, zero padding
     {
