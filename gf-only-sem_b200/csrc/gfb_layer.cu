@@ -82,6 +82,9 @@ __host__ __device__ inline int frame_axis(int frame, int j) {
     return (f < 0 ? -f : f) - 1;
 }
 __host__ __device__ inline float frame_sign(int frame, int j) { return (((frame >> (4 * j)) & 0xf) - 8) < 0 ? -1.f : 1.f; }
+// v[ax] for a runtime axis, by selects (an indexed load would put the
+// array in local memory)
+__device__ inline float pick3(const float* v, int ax) { return ax == 0 ? v[0] : (ax == 1 ? v[1] : v[2]); }
 
 // History of the boundary nodes: ring[slot][b][field][9] global-frame
 // (u, v, a) of one step; state m lives in slot m % 3.
@@ -124,7 +127,7 @@ __device__ inline void node_features(const BNode& bn, int f, int NF, long long n
         for (int ch = 0; ch < 3; ++ch)
 #pragma unroll
             for (int j = 0; j < 3; ++j)
-                x[tap * 9 + ch * 3 + j] = frame_sign(bn.frame, j) * val[ch * 3 + frame_axis(bn.frame, j)] / sc[ch];
+                x[tap * 9 + ch * 3 + j] = frame_sign(bn.frame, j) * pick3(val + ch * 3, frame_axis(bn.frame, j)) / sc[ch];
     }
 }
 
@@ -170,11 +173,17 @@ __device__ inline void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// Warps per block of layer_kernel: every block stages all networks' weights
+// in shared memory once (up to ~180 KB: one block per SM), so the warps of
+// one block are all the warps an SM gets; 12 x 32 threads at ~160 registers
+// fill the register file (the feature gathers need the warps).
+constexpr int kLayerWarps = 12;
+
 template <int NF>
-__global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
+__global__ void __launch_bounds__(kLayerWarps * 32) layer_kernel(LayerArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem_raw);                  // [n_net][kWNet]
-    __nv_bfloat16* sx = sw + (size_t)A.n_net * kWNet;                                 // [4 warps][16][56]
+    __nv_bfloat16* sx = sw + (size_t)A.n_net * kWNet;                                 // [warps][16][56]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     {
         const uint4* src = reinterpret_cast<const uint4*>(A.w);
@@ -208,7 +217,7 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
     const bool on = *((volatile int*)A.active) != 0;
     __nv_bfloat16* xs = sx + warp * 16 * kW1S;
     double work = 0.0, ekin = 0.0;
-    for (int t = blockIdx.x * 4 + warp; t < A.n_tile; t += gridDim.x * 4) {
+    for (int t = blockIdx.x * kLayerWarps + warp; t < A.n_tile; t += gridDim.x * kLayerWarps) {
         const int net = A.tile_net[t];
         const __nv_bfloat16* W = sw + (size_t)net * kWNet;
         // features: lane -> (row lane/2, half lane%2) ... two lanes per sample
@@ -234,11 +243,12 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
 #pragma unroll
             for (int q = 0; q < 9; ++q) cur[q] = 0.f;
         }
-        // half 0 writes k = 0..27, half 1 writes k = 28..55 (zero padding)
+        // half 0 writes k = 0..27, half 1 writes k = 28..55 (zero padding);
+        // both x indices are compile-time, so x stays in registers
 #pragma unroll
         for (int q = 0; q < 28; ++q) {
-            const int k = half * 28 + q;
-            xs[row * kW1S + k] = __float2bfloat16_rn(k < kIn ? x[k] : 0.f);
+            const float hi = q + 28 < kIn ? x[q + 28 < kIn ? q + 28 : 0] : 0.f;
+            xs[row * kW1S + half * 28 + q] = __float2bfloat16_rn(half ? hi : x[q]);
         }
         __syncwarp();
         const int r0 = lane >> 2, c0 = 2 * (lane & 3);
@@ -333,8 +343,11 @@ __global__ void __launch_bounds__(128) layer_kernel(LayerArgs A) {
                     // trapezoidal dashpot: velocity at the end of the step
                     // estimated from this step's force, the damping taken
                     // implicitly, so any sigma >= 0 stays stable
-                    const float vbar = cv[3 + ax] + (float)(0.5 * A.dt) * cv[6 + ax] + hdm * fe[ax];
-                    gc[ax] = -dj * vbar / (1.f + dj * hdm);
+                    const float vbar = pick3(cv + 3, ax) + (float)(0.5 * A.dt) * pick3(cv + 6, ax) + hdm * pick3(fe, ax);
+                    const float gj = -dj * vbar / (1.f + dj * hdm);
+                    gc[0] = ax == 0 ? gj : gc[0];
+                    gc[1] = ax == 1 ? gj : gc[1];
+                    gc[2] = ax == 2 ? gj : gc[2];
                 }
                 const bool fin = isfinite(gc[0]) && isfinite(gc[1]) && isfinite(gc[2]);
                 if (on && fin) {
@@ -482,7 +495,7 @@ gfb_status launch_layer(const SolverView& v, Layer* L) {
     A.monitor = L->monitor;
     A.active = L->active;
     A.threshold = L->threshold;
-    layer_kernel<NF><<<L->blocks, 128, L->smem, v.stream>>>(A);
+    layer_kernel<NF><<<L->blocks, kLayerWarps * 32, L->smem, v.stream>>>(A);
     LCU(cudaGetLastError());
     return GFB_OK;
 }
@@ -801,13 +814,13 @@ gfb_status gfb_layer_attach(gfb_solver* s, const gfb_layer* layer, const uint16_
     const int one = 1;
     LCU(cudaMemcpy(L->active, &one, sizeof(int), cudaMemcpyHostToDevice));
     L->threshold = threshold;
-    L->smem = (size_t)layer->n_net * kWNet * 2 + 4 * 16 * kW1S * 2;
+    L->smem = (size_t)layer->n_net * kWNet * 2 + kLayerWarps * 16 * kW1S * 2;
     if (L->smem > 227 * 1024) return set_error(GFB_ERR_UNSUPPORTED, "learned layer: too many networks");
     int n_sm = 0, per_sm = 0;
     LCU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, v.device));
     auto set = [&](auto kern) -> gfb_status {
         LCU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem));
-        LCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, L->smem));
+        LCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLayerWarps * 32, L->smem));
         return GFB_OK;
     };
     if (v.n_field == 1) st = set(layer_kernel<1>);
@@ -815,7 +828,7 @@ gfb_status gfb_layer_attach(gfb_solver* s, const gfb_layer* layer, const uint16_
     else st = set(layer_kernel<3>);
     if (st) return st;
     if (per_sm < 1) return set_error(GFB_ERR_UNSUPPORTED, "learned layer: kernel does not fit on an SM");
-    L->blocks = std::max(1, std::min(per_sm * n_sm, (L->B.n_tile + 3) / 4));
+    L->blocks = std::max(1, std::min(per_sm * n_sm, (L->B.n_tile + kLayerWarps - 1) / kLayerWarps));
     return solver_set_layer(s, L.release());
 }
 
