@@ -628,7 +628,10 @@ def run_gfb(args):
         import torch.distributed as tdist
 
         torch.cuda.set_device(local)
-        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        # every rank does the same work between collectives (input generation,
+        # create, the timed steps), so a rank that is minutes late has failed:
+        # a short timeout ends the others with an error instead of a hang
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=180))
         dist = tdist
     device = local if world > 1 else args.device
     prec = gfb.FP32 if args.precision == "fp32" else gfb.FP64
