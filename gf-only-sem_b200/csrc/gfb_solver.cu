@@ -893,65 +893,55 @@ gfb_status spill(gfb_solver* s, Snapshot& snap) {
 // C-PML at global nodes: B_k = sum over C-PML cells at the node of
 // w J/rho A_k (k = 1..5, accumulated in FP64 in cell order), and for each
 // axis the convolution coefficients of the cells where that axis acts.
-// Returns false (per-cell form) if two cells disagree on an axis's
-// coefficients at a shared node (beyond 1e-6 relative).  slot[g] numbers the C-PML nodes in
-// increasing node order; coef is [slot][14].
-bool plan_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w, const NodeBuckets& nb,
-                   std::vector<int>& slot, std::vector<double>& coef) {
+// live_pts[t]: the live C-PML points (some A_k != 0) of owner t's nodes in
+// increasing point order, so each owner thread accumulates its nodes in mesh
+// order; the slot of node g is its device index (the C-PML nodes are the
+// first n_slot device nodes); coef is [slot][14].  Returns false (per-cell
+// form) if two cells disagree on an axis's coefficients at a shared node
+// (beyond 1e-6 relative).
+bool accumulate_node_pml(const gfb_solver* s, const gfb_mesh* m, const std::vector<double>& w,
+                         const std::vector<std::vector<long long>>& live_pts, int n_slot, std::vector<double>& coef) {
     const int ng = s->ng, nn = s->nn;
-    auto live = [&](long long q) {
-        if (m->pml_region[q / nn] == 0) return false;
-        const double* A = m->pml_coef_abar + q * 5;
-        return A[0] != 0.0 || A[1] != 0.0 || A[2] != 0.0 || A[3] != 0.0 || A[4] != 0.0;
-    };
-    // each thread goes through the points of its own nodes in mesh order,
-    // so every node accumulates in the same order as one pass would
-    slot.assign(s->n_node, -1);
-    nb.for_each_owner([&](int, long long, long long, const long long* qs, size_t nq) {
-        for (size_t k = 0; k < nq; ++k)
-            if (live(qs[k])) slot[m->ibool[qs[k]]] = 0;
-    });
-    int n = 0;
-    for (int g = 0; g < s->n_node; ++g)
-        if (slot[g] >= 0) slot[g] = n++;
-    coef.assign((size_t)n * 14, 0.0);
-    std::vector<unsigned char> have(n, 0);
+    coef.assign((size_t)n_slot * 14, 0.0);
+    std::vector<unsigned char> have(n_slot, 0);
     std::atomic<bool> agree(true);
-    nb.for_each_owner([&](int, long long, long long, const long long* qs, size_t nq) {
-        for (size_t k = 0; k < nq; ++k) {
-            const long long q = qs[k];
-            if (!live(q)) continue;
-            const int p = (int)(q % nn);
-            const double* A = m->pml_coef_abar + q * 5;
-            const int sl = slot[m->ibool[q]];
-            double* c = &coef[(size_t)sl * 14];
-            const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
-            const double wgll = w[ni] * w[nj] * w[nk];
-            const double rho = m->density[q];
-            const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
-            for (int kk = 0; kk < 5; ++kk) c[kk] += scale * A[kk];
-            const double* al = m->pml_coef_alpha + q * 9;
-            for (int ax = 0; ax < 3; ++ax) {
-                if (A[2 + ax] == 0.0) continue;
-                if (!(have[sl] & (1u << ax))) {
-                    for (int t = 0; t < 3; ++t) c[5 + ax * 3 + t] = al[ax * 3 + t];
-                    have[sl] |= (unsigned char)(1u << ax);
-                } else {
-                    for (int t = 0; t < 3; ++t) {
-                        const double a0 = c[5 + ax * 3 + t], a1 = al[ax * 3 + t];
-                        // the cells' coefficients at a node come from the same position
-                        // through different cell maps: equal up to rounding (seen up to
-                        // ~1e-9 relative on deformed meshes); different profiles differ
-                        // at O(1)
-                        if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) {
-                            agree.store(false);
-                            return;
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < live_pts.size(); ++t)
+        th.emplace_back([&, t] {
+            for (const long long q : live_pts[t]) {
+                const int p = (int)(q % nn);
+                const double* A = m->pml_coef_abar + q * 5;
+                const int g = m->ibool[q];
+                const int sl = s->node_inv.empty() ? g : s->node_inv[g];
+                double* c = &coef[(size_t)sl * 14];
+                const int nk = p % ng, nj = (p / ng) % ng, ni = p / (ng * ng);
+                const double wgll = w[ni] * w[nj] * w[nk];
+                const double rho = m->density[q];
+                const double scale = wgll * ((rho > 0.0) ? 1.0 / rho : 0.0) * m->jacobian[q];
+                for (int kk = 0; kk < 5; ++kk) c[kk] += scale * A[kk];
+                const double* al = m->pml_coef_alpha + q * 9;
+                for (int ax = 0; ax < 3; ++ax) {
+                    if (A[2 + ax] == 0.0) continue;
+                    if (!(have[sl] & (1u << ax))) {
+                        for (int k = 0; k < 3; ++k) c[5 + ax * 3 + k] = al[ax * 3 + k];
+                        have[sl] |= (unsigned char)(1u << ax);
+                    } else {
+                        for (int k = 0; k < 3; ++k) {
+                            const double a0 = c[5 + ax * 3 + k], a1 = al[ax * 3 + k];
+                            // the cells' coefficients at a node come from the same position
+                            // through different cell maps: equal up to rounding (seen up to
+                            // ~1e-9 relative on deformed meshes); different profiles differ
+                            // at O(1)
+                            if (std::abs(a0 - a1) > 1e-6 * std::max(std::abs(a0), std::abs(a1))) {
+                                agree.store(false);
+                                return;
+                            }
                         }
                     }
                 }
             }
-        }
-    });
+        });
+    for (auto& x : th) x.join();
     return agree.load();
 }
 
@@ -989,7 +979,8 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
                         const gfb_model* models, const std::vector<int>& perm, const std::vector<int>& inv_perm,
                         const std::vector<uint32_t>& ibool_dev, const std::vector<double>& node_mass,
                         const std::vector<double>& node_damp, const std::vector<long long>& first_q,
-                        std::vector<uint8_t>& first_flag, const NodeBuckets& nb, const std::vector<double>& w,
+                        std::vector<uint8_t>& first_flag, const std::vector<uint8_t>& node_live,
+                        const std::vector<std::vector<long long>>& live_pts, const std::vector<double>& w,
                         const std::vector<double>& D, StageClock& clk) {
     const int ng = s->ng, nn = s->nn;
     const long long n_cell = s->n_cell;
@@ -1034,25 +1025,19 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
     // and of its neighbours sit close in memory whatever the input
     // numbering (the reference's coordinate sort scatters them on deformed
     // meshes)
-    std::vector<int> pslot;
-    std::vector<double> pcoef;
-    const bool node_form = s->has_cpml && s->prec == GFB_FP32 && !(s->flags & GFB_FLAG_CELL_PML) &&
-                           plan_node_pml(s, m, w, nb, pslot, pcoef);
-    clk.mark("C-PML node plan");
-    {
-        // first_flag[q]: 1 if q is its node's first touch, 2 if that node is
-        // also a node-form C-PML node
+    // first_flag[q]: 1 if q is its node's first touch, 2 if that node is a
+    // live C-PML node numbered first
+    auto number_nodes = [&](bool pml_first) {
         s->node_perm.clear();
         s->node_inv.clear();
         s->node_perm.reserve(s->n_node);
         const long long P = n_cell * nn;
-        if (node_form)
-            parallel_for(s->n_node, [&](long long g0, long long g1) {
-                for (long long g = g0; g < g1; ++g)
-                    if (pslot[g] >= 0) first_flag[first_q[g]] = 2;
-            });
+        parallel_for(s->n_node, [&](long long g0, long long g1) {
+            for (long long g = g0; g < g1; ++g)
+                if (first_q[g] >= 0) first_flag[first_q[g]] = (pml_first && node_live[g]) ? 2 : 1;
+        });
         auto node_of = [&](long long q) { return m->ibool[q]; };
-        for (int pass = node_form ? 0 : 1; pass < 2; ++pass) {
+        for (int pass = pml_first ? 0 : 1; pass < 2; ++pass) {
             const uint8_t want = pass == 0 ? 2 : 1;
             parallel_compact(P, [&](long long q) { return first_flag[q] == want; }, node_of, s->node_perm);
         }
@@ -1074,21 +1059,25 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
                 for (long long d = d0; d < d1; ++d) s->node_inv[s->node_perm[d]] = (int)d;
             });
         }
-        if (node_form) {
-            // slots follow the device order
-            const int n_slot = (int)(pcoef.size() / 14);
-            std::vector<double> c2(pcoef.size());
-            parallel_for(n_slot, [&](long long d0, long long d1) {
-                for (long long d = d0; d < d1; ++d) {
-                    const int g = s->node_perm.empty() ? (int)d : s->node_perm[d];
-                    std::copy(pcoef.begin() + (size_t)pslot[g] * 14, pcoef.begin() + (size_t)pslot[g] * 14 + 14,
-                              c2.begin() + (size_t)d * 14);
-                }
-            });
-            pcoef.swap(c2);
+    };
+    // node-form C-PML (FP32 path): its nodes are numbered first and its
+    // coefficients accumulated straight into their device slots; if two
+    // cells disagree at a node, the per-cell form is used and the nodes are
+    // numbered again without the C-PML group
+    bool node_form = !node_live.empty();
+    number_nodes(node_form);
+    clk.mark("node numbering");
+    std::vector<double> pcoef;
+    if (node_form) {
+        long long n_live = 0;
+        for (size_t g = 0; g < node_live.size(); ++g) n_live += node_live[g];
+        if (!accumulate_node_pml(s, m, w, live_pts, (int)n_live, pcoef)) {
+            node_form = false;
+            pcoef.clear();
+            number_nodes(false);
         }
     }
-    clk.mark("node numbering");
+    clk.mark("C-PML node plan");
     auto dev_node = [&](long long g) -> long long { return s->node_inv.empty() ? g : s->node_inv[g]; };
     // ibool in device node numbers, and the rows of the pipelined kernels:
     // node words, then the cell's model, zero padding
@@ -1690,7 +1679,12 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     std::vector<double> node_mass(m->n_node, 0.0), node_damp(m->n_node, 0.0);
     std::vector<long long> first_q(m->n_node, -1);
     std::vector<uint8_t> first_flag((size_t)P, 0);  // 1: the point is its node's first touch
-    nb.for_each_owner([&](int, long long, long long, const long long* qs, size_t nq) {
+    // the FP32 path keeps C-PML per node when it can: the same pass marks
+    // the live C-PML points (some A_k != 0 in a C-PML cell) and their nodes
+    const bool want_node_pml = s->has_cpml && s->prec == GFB_FP32 && !(c->flags & GFB_FLAG_CELL_PML);
+    std::vector<uint8_t> node_live(want_node_pml ? (size_t)m->n_node : 0, 0);
+    std::vector<std::vector<long long>> live_pts(want_node_pml ? nb.n_owner : 0);
+    nb.for_each_owner([&](int t, long long, long long, const long long* qs, size_t nq) {
         for (size_t k = 0; k < nq; ++k) {
             const long long q = qs[k];
             const int g = m->ibool[q];
@@ -1699,6 +1693,13 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
             if (first_q[g] < 0) {
                 first_q[g] = q;
                 first_flag[q] = 1;
+            }
+            if (want_node_pml && m->pml_region[q / nn] != 0) {
+                const double* A = m->pml_coef_abar + q * 5;
+                if (A[0] != 0.0 || A[1] != 0.0 || A[2] != 0.0 || A[3] != 0.0 || A[4] != 0.0) {
+                    node_live[g] = 1;
+                    live_pts[t].push_back(q);
+                }
             }
         }
     });
@@ -1761,11 +1762,11 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     if (s->prec == GFB_FP64) {
         if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<double>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                  first_q, first_flag, nb, w, D, clk);
+                                  first_q, first_flag, node_live, live_pts, w, D, clk);
     } else {
         if ((st = dispatch<float, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<float>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
-                                 first_q, first_flag, nb, w, D, clk);
+                                 first_q, first_flag, node_live, live_pts, w, D, clk);
     }
     if (st) return st;
     CU(cudaStreamSynchronize(s->stream));
