@@ -16,6 +16,7 @@
 //
 // The array is kScratchBytes (8 MiB) per GPU; every GPU that loads this
 // library holds it until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -37,7 +38,49 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 256;
 std::mutex g_scratch_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_scratch per device, with the id of the CUDA context it
+// was looked up in.  A device reset (cudaDeviceReset, or the primary context
+// released and created again) loads the library's device code into a new
+// context, where the array can sit at another address; the id tells the
+// contexts apart, so the address is looked up again in the new one.
+struct ScratchAddr {
+    bool valid = false;
+    unsigned long long ctx_id = 0;
+    void* addr = nullptr;
+};
+ScratchAddr g_scratch_addr[kMaxDevices];
+
+// Driver entry points for the current context and its id, fetched through
+// the runtime (the library does not link the driver library itself).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+bool current_context_id(int dev, unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return false;
+    if (!ctx) {
+        // no context bound to this host thread yet: bind the device's
+        // primary context (the one the runtime launches into)
+        if (cudaSetDevice(dev) != cudaSuccess || get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    }
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
@@ -57,12 +100,18 @@ Layout layout_for(long long n_elem, int ngll) {
     return L;
 }
 
-// Device address of g_scratch on the current device, looked up on the first
-// call for that device.
+// Device address of g_scratch on the current device dev: looked up with
+// cudaGetSymbolAddress on the first call in each CUDA context of the device
+// (the first call on the device, and the first after a device reset), and
+// taken from the cache otherwise.  If the driver cannot report the
+// context's id, the address is looked up on every call.
 gfb_status scratch_on_device(int dev, unsigned char** out) {
     if (dev < 0 || dev >= kMaxDevices) return gfb::set_error(GFB_ERR_INVALID, "device ordinal out of range");
+    unsigned long long ctx_id = 0;
+    const bool have_id = current_context_id(dev, &ctx_id);
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
+    ScratchAddr& c = g_scratch_addr[dev];
+    if (!have_id || !c.valid || c.ctx_id != ctx_id) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess) {
@@ -71,9 +120,11 @@ gfb_status scratch_on_device(int dev, unsigned char** out) {
                      cudaGetErrorString(e));
             return gfb::set_error(GFB_ERR_CUDA, msg);
         }
-        g_scratch_addr[dev] = p;
+        c.addr = p;
+        c.ctx_id = ctx_id;
+        c.valid = have_id;
     }
-    *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    *out = static_cast<unsigned char*>(c.addr);
     return GFB_OK;
 }
 
@@ -118,6 +169,13 @@ gfb_status run(int n_elem, const double* dxi_dx, const double* jacobian, const d
     const long long total = (long long)n_elem * S::NN;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
     repack_kernel<NG><<<blocks, 256, 0, stream>>>(n_elem, dxi_dx, jacobian, lambda_, mu, t, geom, ibool, dmat);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        char msg[256];
+        snprintf(msg, sizeof(msg), "element residual (no-alloc): repack kernel launch failed: %s",
+                 cudaGetErrorString(e));
+        return gfb::set_error(GFB_ERR_CUDA, msg);
+    }
     gfb::ElemArgs<double> A{};
     A.e_begin = 0;
     A.e_end = n_elem;
@@ -132,10 +190,11 @@ gfb_status run(int n_elem, const double* dxi_dx, const double* jacobian, const d
     const int eblocks = (n_elem + S::EPB - 1) / S::EPB;
     gfb::elem_step_kernel<double, NG, 1>
         <<<eblocks, S::THREADS, gfb::elem_smem_bytes<double, NG, 1>(), stream>>>(A);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) {
         char msg[256];
-        snprintf(msg, sizeof(msg), "element kernel launch failed: %s", cudaGetErrorString(e));
+        snprintf(msg, sizeof(msg), "element residual (no-alloc): element kernel launch failed: %s",
+                 cudaGetErrorString(e));
         return gfb::set_error(GFB_ERR_CUDA, msg);
     }
     return GFB_OK;
@@ -174,6 +233,10 @@ gfb_status gfb_element_residual_noalloc(int32_t n_elem, const double* dxi_dx, co
                  n_elem, max_cells, ngll, kScratchBytes);
         return gfb::set_error(GFB_ERR_INVALID, msg);
     }
+    // an error left by an earlier, unrelated call would otherwise be read
+    // back after this call's launches and reported as theirs: clear it (a
+    // sticky error of a broken context comes back at the launches anyway)
+    (void)cudaGetLastError();
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return gfb::set_error(GFB_ERR_NO_DEVICE, "no current CUDA device");

@@ -1565,6 +1565,20 @@ extern "C" {
 
 int32_t gfb_abi_version(void) { return GFB_ABI_VERSION; }
 
+gfb_status gfb_kernel_arch(int32_t device, int32_t* binary_version, int32_t* ptx_version) {
+    if (!binary_version || !ptx_version) return fail(GFB_ERR_INVALID, "kernel arch: NULL output");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(GFB_ERR_NO_DEVICE, "no CUDA-capable GPU found");
+    if (device < 0 || device >= ndev) return fail(GFB_ERR_INVALID, "device %d not present", device);
+    CU(cudaSetDevice(device));
+    cudaFuncAttributes fa{};
+    CU(cudaFuncGetAttributes(&fa, gfb::predict_kernel<float>));
+    *binary_version = fa.binaryVersion;
+    *ptx_version = fa.ptxVersion;
+    return GFB_OK;
+}
+
 const char* gfb_last_error(void) { return g_err.c_str(); }
 
 }  // extern "C"
@@ -1592,8 +1606,11 @@ bool greedy_colour(const gfb_mesh* m, int nn, std::vector<T>& used, std::vector<
     return true;
 }
 
+// w_tab / D_tab: GLL weights [ngll] and derivative matrix [ngll*ngll] to use
+// instead of the tables computed from ngll (NULL: computed).
 gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, int n_model,
-                       const gfb_model* models, gfb_solver** out) {
+                       const gfb_model* models, gfb_solver** out, const double* w_tab = nullptr,
+                       const double* D_tab = nullptr) {
     gfb_status st;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -1759,6 +1776,8 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     clk.mark("colour order");
     std::vector<double> x, w, D;
     if (!gll_tables(m->ngll - 1, x, w, D)) return fail(GFB_ERR_INVALID, "GLL table construction failed");
+    if (w_tab) w.assign(w_tab, w_tab + m->ngll);
+    if (D_tab) D.assign(D_tab, D_tab + (size_t)m->ngll * m->ngll);
     if (s->prec == GFB_FP64) {
         if ((st = dispatch<double, SmemOp>(s->ng, s->nfld, s.get()))) return st;
         st = build_device<double>(s.get(), m, src, n_model, models, perm, inv_perm, ibool_dev, node_mass, node_damp,
@@ -2252,8 +2271,6 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
     if (n_elem <= 0 || !dxi_dx || !jacobian || !lambda_ || !mu || !u || !r)
         return fail(GFB_ERR_INVALID, "element residual: missing input");
     if (ngll < 3 || ngll > 6) return fail(GFB_ERR_UNSUPPORTED, "ngll=%d outside 3..6", ngll);
-    (void)D;
-    (void)weights;  // tables are rebuilt from ngll (same values as gll.hpp)
     const int nn = ngll * ngll * ngll;
     const long long P = (long long)n_elem * nn;
     if (P >= (long long)gfb::kNodeMask) return fail(GFB_ERR_INVALID, "too many element nodes");
@@ -2279,8 +2296,16 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
     c.device = device;
     c.record_slots = 1;
     gfb_solver* s = nullptr;
-    gfb_status st = gfb_create(&m, &c, nullptr, &s);
+    gfb_status st = validate(&m, &c);
     if (st) return st;
+    gfb_model one{};
+    one.cell_end = n_elem;
+    one.node_end = m.n_node;
+    one.dt = c.dt;
+    one.n_steps = INT32_MAX;
+    // the caller's GLL tables, as compute_element_residual uses the tables
+    // it is given (element_cpu.cpp:19-162); NULL selects the GLL tables of ngll
+    if ((st = create_impl(&m, &c, nullptr, 1, &one, &s, weights, D))) return st;
     std::unique_ptr<gfb_solver, gfb_status (*)(gfb_solver*)> guard(s, gfb_destroy);
     // [point][4] padded vectors on the device
     const size_t nP = (size_t)P * 4;

@@ -126,6 +126,11 @@ typedef struct gfb_solver gfb_solver;
 /* ABI version of the loaded library (compare with GFB_ABI_VERSION). */
 int32_t gfb_abi_version(void);
 
+/* Architecture the library's device code was built for, as the CUDA runtime
+ * reports it for one of its kernels on `device` (cudaFuncGetAttributes):
+ * binary_version 100 is sm_100 (sm_100a).  No counterpart in the reference. */
+gfb_status gfb_kernel_arch(int32_t device, int32_t* binary_version, int32_t* ptx_version);
+
 /* Message of the last failing call on this thread ("" if none). */
 const char* gfb_last_error(void);
 
@@ -310,7 +315,9 @@ gfb_status gfb_read_record_f32(gfb_solver* solver, int32_t field, int32_t* step,
  * Element internal force for n_elem independent elements, host arrays in
  * and out (r is overwritten with K_e u).  Replaces
  * compute_element_residual<BackendCUDA> (element.hpp:39-42,
- * element_cuda.cu:195-252); D and weights are the GLL tables of ngll.
+ * element_cuda.cu:195-252).  D [ngll*ngll] (D[i*ngll+j] = l_j'(x_i)) and
+ * weights [ngll] are used as given, as the reference uses the tables it is
+ * passed; either may be NULL to use the GLL tables of ngll.
  * precision selects the FP64 or FP32 kernel.
  */
 gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const double* jacobian,
@@ -339,8 +346,10 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
  * process exits.  n_elem is limited to what fits: 3106 cells at ngll=3,
  * 1310 at ngll=4, 671 at ngll=5, 388 at ngll=6; larger calls are rejected
  * with GFB_ERR_INVALID and a message giving the maximum (split the call).
- * The first call on a device looks up the array's device address; make
- * that first call before any CUDA stream capture.  All calls on a device
+ * The first call on a device looks up the array's device address, and so
+ * does the first call after a device reset (cudaDeviceReset, or the
+ * primary context released and created again), where the array can move;
+ * make those calls before any CUDA stream capture.  All calls on a device
  * share the one array and each call rewrites the part it reads, so calls
  * that may overlap on the GPU (different streams, or host threads without
  * ordering) race; serialise them on one stream.  FP64 only.

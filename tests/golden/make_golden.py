@@ -1,6 +1,7 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference) and
+Run in a container that has the reference tree (its path as the first
+argument, or GF_REFERENCE_ROOT, else /root/reference) and
 the oracle built (``make -C oracle``):
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -197,7 +198,7 @@ def make_case(R, name: str, c: dict):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GF_REFERENCE_ROOT", "/root/reference")
     R = import_reference(ref_root)
     for name, c in CASES.items():
         make_case(R, name, c)
