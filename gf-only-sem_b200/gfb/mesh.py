@@ -70,6 +70,21 @@ CPML_XY_ONLY, CPML_XZ_ONLY, CPML_YZ_ONLY, CPML_XYZ = 4, 5, 6, 7
 # ---------------------------------------------------------------------------
 
 
+def for_chunks(fn, starts, threads: int = 1):
+    """fn(start) for every start; on ``threads`` host threads when > 1 (numpy
+    releases the interpreter lock in its array loops and matrix products)."""
+    starts = list(starts)
+    if threads <= 1 or len(starts) <= 1:
+        for c0 in starts:
+            fn(c0)
+        return
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for _ in ex.map(fn, starts):
+            pass
+
+
 def _legendre(n: int, x):
     x = np.asarray(x, dtype=np.float64)
     if n == 0:
@@ -213,11 +228,12 @@ def cell_corners(spec: MeshSpec, V: np.ndarray) -> np.ndarray:
     return out
 
 
-def gll_geometry(corners: np.ndarray, order: int, chunk: int = 65536):
+def gll_geometry(corners: np.ndarray, order: int, chunk: int = 65536, threads: int = 1):
     """coords, jacobian (det J), dxi_dx (inv(J) raveled), geometric mass.
 
-    Same trilinear map as gll_geometry.py:160-184, vectorised over cells.
-    """
+    Same trilinear map as gll_geometry.py:160-184, vectorised over cells;
+    ``threads`` > 1 processes chunks of cells on that many host threads (the
+    per-cell arithmetic, hence every value, is the same)."""
     pts = gll_points(order)
     w = gll_weights(pts)
     ng = order + 1
@@ -237,7 +253,8 @@ def gll_geometry(corners: np.ndarray, order: int, chunk: int = 65536):
     dxi = np.empty((n_cell, nn, 9))
     # shape-function products as matrix products over all cells of a chunk
     dSm = np.ascontiguousarray(dS.transpose(0, 2, 1).reshape(nn * 3, 8))  # [(n, m), a]
-    for c0 in range(0, n_cell, chunk):
+
+    def one(c0):
         cv = corners[c0 : c0 + chunk]
         ne = cv.shape[0]
         xa = np.ascontiguousarray(cv.transpose(1, 0, 2).reshape(8, ne * 3))  # [a, (e, c)]
@@ -260,6 +277,8 @@ def gll_geometry(corners: np.ndarray, order: int, chunk: int = 65536):
         inv[..., 3], inv[..., 4], inv[..., 5] = B * rdet, (a * i - c * g) * rdet, (c * d - a * f) * rdet
         inv[..., 6], inv[..., 7], inv[..., 8] = C * rdet, (b * g - a * h) * rdet, (a * e - b * d) * rdet
         dxi[c0 : c0 + chunk] = inv
+
+    for_chunks(one, range(0, n_cell, chunk), threads)
     wijk = (w[:, None, None] * w[None, :, None] * w[None, None, :]).ravel()
     mass = jac * wijk[None, :]
     return (
@@ -505,7 +524,28 @@ def abar_coefficients(K, d, al, regions):
     return out
 
 
-def cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt):
+def cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt, threads: int = 1, chunk: int = 65536):
+    """Region, coef_alpha [n_cell, nn, 9] and A1..A5 [n_cell, nn, 5]; every
+    value depends on its own cell only, so ``threads`` > 1 computes chunks of
+    cells on that many host threads with the same arithmetic."""
+    n_cell = coords.shape[0]
+    if threads <= 1 or n_cell <= chunk:
+        return _cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt)
+    nn = int(np.prod(coords.shape[1:-1]))
+    region = np.empty(n_cell, dtype=np.int32)
+    calpha = np.empty((n_cell, nn, 9))
+    abar = np.empty((n_cell, nn, 5))
+
+    def one(c0):
+        sl = slice(c0, c0 + chunk)
+        r, ca, ab = _cpml_parameters(coords[sl], is_pml[sl], bounds, widths, vp[sl], f0, dt)
+        region[sl], calpha[sl], abar[sl] = r, ca, ab
+
+    for_chunks(one, range(0, n_cell, chunk), threads)
+    return region, calpha, abar
+
+
+def _cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt):
     regions = cpml_regions(coords, is_pml, bounds, widths)
     K, d, al = cpml_profiles(coords, is_pml, regions, bounds, widths, vp, f0)
     n_cell, nn = K.shape[0], K.shape[1]
@@ -628,14 +668,21 @@ def ricker(t, f0=2.0, t0=1.0, amp=1.0e20):
     return amp * (1.0 - 2.0 * a**2) * np.exp(-(a**2))
 
 
-def h_min(coords: np.ndarray) -> float:
+def h_min(coords: np.ndarray, threads: int = 1, chunk: int = 65536) -> float:
     """Smallest distance between adjacent GLL nodes of any cell (cfl_validator.py:38-62)."""
-    best = np.inf
-    for ax in (1, 2, 3):
-        a = np.take(coords, np.arange(1, coords.shape[ax]), axis=ax)
-        b = np.take(coords, np.arange(0, coords.shape[ax] - 1), axis=ax)
-        best = min(best, float(np.sqrt(((a - b) ** 2).sum(-1)).min()))
-    return best
+    out = {}
+
+    def one(c0):
+        c = coords[c0 : c0 + chunk]
+        best = np.inf
+        for ax in (1, 2, 3):
+            a = np.take(c, np.arange(1, c.shape[ax]), axis=ax)
+            b = np.take(c, np.arange(0, c.shape[ax] - 1), axis=ax)
+            best = min(best, float(np.sqrt(((a - b) ** 2).sum(-1)).min()))
+        out[c0] = best
+
+    for_chunks(one, range(0, coords.shape[0], chunk), threads)
+    return min(out.values()) if out else np.inf
 
 
 # ---------------------------------------------------------------------------
@@ -730,17 +777,39 @@ def build_problem(
     with_cpml: bool = True,
     record_tile=None,
     device: Optional[int] = None,
+    numbering_device: Optional[int] = None,
+    threads: int = 1,
+    cell_window=None,
+    require_source: bool = True,
 ) -> dict:
     """Every solver input for one synthetic model, reference layouts.
 
     ``device`` = a GPU index computes the GLL geometry, the node numbering
-    and the C-PML coefficients there (``gfb.prep``) instead of on the host."""
-    if device is not None:
+    and the C-PML coefficients there (``gfb.prep``) instead of on the host.
+    ``numbering_device`` = a GPU index numbers the host-computed points there
+    (the same ids as the host's lexsort of the same points, partition.py's
+    rule, in a fraction of the time).  ``threads`` = host threads for the
+    per-cell host stages (same values for any count).  ``cell_window`` =
+    (i0, i1, j0, j1, k0, k1) keeps only the cells with i0 <= i < i1,
+    j0 <= j < j1, k0 <= k < k1 of the full mesh (x fastest), a piece of the
+    model with the full model's vertices, bounds and C-PML layers.  With
+    ``require_source`` False a source outside every non-C-PML cell leaves the
+    model without a source instead of raising."""
+    if device is not None or numbering_device is not None:
         from . import prep
     V = vertex_grid(spec)
     corners = cell_corners(spec, V)
+    is_pml = pml_flags(spec)
+    n_cell = spec.n_cell
+    if cell_window is not None:
+        i0, i1, j0, j1, k0, k1 = cell_window
+        if record_tile is not None:
+            raise ValueError("a recording tile is defined on the full mesh")
+        k, j, i = np.meshgrid(np.arange(k0, k1), np.arange(j0, j1), np.arange(i0, i1), indexing="ij")
+        sel = (i.ravel() + spec.nx * (j.ravel() + spec.ny * k.ravel())).astype(np.int64)
+        corners, is_pml, n_cell = corners[sel], is_pml[sel], int(sel.size)
     if device is None:
-        coords, jac, dxi, mgeo = gll_geometry(corners, spec.order)
+        coords, jac, dxi, mgeo = gll_geometry(corners, spec.order, threads=threads)
     else:
         coords, jac, dxi, mgeo = prep.gll_geometry(corners, spec.order, device=device)
     bounds = {
@@ -751,14 +820,22 @@ def build_problem(
         "zmin": float(V[..., 2].min()),
         "zmax": float(V[..., 2].max()),
     }
-    vp, vs, rho = material(coords)
+    if threads > 1:
+        vp, vs, rho = (np.empty(coords.shape[:-1]) for _ in range(3))
+
+        def mat(c0, n=65536):
+            vp[c0 : c0 + n], vs[c0 : c0 + n], rho[c0 : c0 + n] = material(coords[c0 : c0 + n])
+
+        for_chunks(mat, range(0, coords.shape[0], 65536), threads)
+    else:
+        vp, vs, rho = material(coords)
     mu = rho * vs**2
     lam = rho * (vp**2 - 2.0 * vs**2)
     mass = mgeo * rho
     if dt is None:
-        dt = cfl * h_min(coords) / float(vp.max())
-    is_pml = pml_flags(spec)
-    ibool, n_node = global_numbering(coords) if device is None else prep.global_numbering(coords, device=device)
+        dt = cfl * h_min(coords, threads=threads) / float(vp.max())
+    ndev = device if device is not None else numbering_device
+    ibool, n_node = global_numbering(coords) if ndev is None else prep.global_numbering(coords, device=ndev)
     widths = {
         "xmin": spec.pml.get("xmin", 0) * (bounds["xmax"] - bounds["xmin"]) / spec.nx,
         "xmax": spec.pml.get("xmax", 0) * (bounds["xmax"] - bounds["xmin"]) / spec.nx,
@@ -770,7 +847,7 @@ def build_problem(
     out = {
         "spec": spec,
         "ngll": spec.order + 1,
-        "n_cell": spec.n_cell,
+        "n_cell": n_cell,
         "n_node": n_node,
         "bounds": bounds,
         "coords": coords,
@@ -783,7 +860,7 @@ def build_problem(
         "lambda": lam,
         "mu": mu,
         "ibool": ibool,
-        "cell_ids": np.arange(spec.n_cell, dtype=np.int64),
+        "cell_ids": np.arange(n_cell, dtype=np.int64),
         "is_pml": is_pml,
         "dt": float(dt),
         "nsteps": int(nsteps),
@@ -791,7 +868,7 @@ def build_problem(
     }
     if with_cpml:
         if device is None:
-            region, calpha, abar = cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt)
+            region, calpha, abar = cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt, threads=threads)
         else:
             region, calpha, abar = prep.cpml_parameters(coords, is_pml, bounds, widths, vp, f0, dt, device=device)
         out["pml_region"] = region
@@ -800,7 +877,13 @@ def build_problem(
         out["damping"] = np.zeros(coords.shape[:4])
     else:
         out["damping"] = legacy_damping(spec, coords, bounds, is_pml)
-    src_ids, src_w = locate_point_source(coords, corners, source_xyz, is_pml, spec.order)
+    try:
+        src_ids, src_w = locate_point_source(coords, corners, source_xyz, is_pml, spec.order)
+    except ValueError:
+        if require_source:
+            raise
+        ng = spec.order + 1
+        src_ids, src_w = np.zeros(0, dtype=np.int64), np.zeros((0, ng, ng, ng))
     out["src_cell_ids"] = src_ids
     out["src_weights"] = src_w
     t = np.arange(nsteps) * dt
