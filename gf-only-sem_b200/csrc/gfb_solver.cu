@@ -1565,6 +1565,14 @@ extern "C" {
 
 int32_t gfb_abi_version(void) { return GFB_ABI_VERSION; }
 
+gfb_status gfb_device_count(int32_t* n) {
+    if (!n) return fail(GFB_ERR_INVALID, "device count: NULL output");
+    int k = 0;
+    if (cudaGetDeviceCount(&k) != cudaSuccess) k = 0;
+    *n = k;
+    return GFB_OK;
+}
+
 gfb_status gfb_kernel_arch(int32_t device, int32_t* binary_version, int32_t* ptx_version) {
     if (!binary_version || !ptx_version) return fail(GFB_ERR_INVALID, "kernel arch: NULL output");
     int ndev = 0;
@@ -2334,17 +2342,6 @@ gfb_status gfb_element_residual(int32_t n_elem, const double* dxi_dx, const doub
             for (int c = 0; c < 3; ++c) r[q * 3 + c] = h[q * 4 + c];
     }
     return GFB_OK;
-}
-
-int32_t gfb_run_forward(const char* direction, int32_t resume, int32_t effective_nprocs) {
-    (void)resume;
-    (void)effective_nprocs;
-    if (!direction || (strcmp(direction, "x") && strcmp(direction, "y") && strcmp(direction, "z"))) {
-        fail(GFB_ERR_INVALID, "--direction must be x, y, or z");
-        return 1;
-    }
-    fail(GFB_ERR_IO, "the library was built without an HDF5 reader for config.h5 / partition_{r}.h5");
-    return 1;
 }
 
 }  // extern "C"

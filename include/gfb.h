@@ -493,11 +493,40 @@ gfb_status gfb_prep_cpml(int32_t device, int64_t n_cell, int32_t ngll, const dou
                          double log_r, int32_t* region, double* coef_alpha, double* abar);
 
 /*
- * File-level driver: run the forward solve of one direction with the
- * reference's CWD-relative file contract (solver.cpp:73-739,
- * main.cpp:32-137).  Returns 0 on success, 1 on failure, like run_forward.
+ * File-level driver: the forward solve of one direction with the
+ * reference's working-directory file contract (run_forward,
+ * forward/share/src/solver.cpp:73-739; the CLI of main.cpp:32-137 is the
+ * gf_solver_elastic_cuda executable over this call).  Reads config.<ext>
+ * and every partitions/partition_{r}.<ext> (merged onto one GPU as
+ * read_partition_all does, io.cpp:319-450), writes
+ * wavefields/{dir}/record_0_{step}.<ext> per snapshot with the datasets
+ * and attributes of RecordWriter::write_step (record.cpp:175-257),
+ * wavefields/{dir}/restart_0.<ext> (restart.cpp:87-139) and
+ * log/forward_{dir}_0.log (logger.hpp:23-30).  <ext> is h5 in a build with
+ * HDF5 when config.h5 exists, else gfr: a raw container holding the same
+ * dataset and attribute names (layout in csrc/gfb_files.h).  With resume,
+ * the state of wavefields/{dir}/restart_0.<ext> is loaded before the file
+ * is recreated.  The environment variable GFB_PRECISION=fp32 selects the
+ * FP32 path (FP64 otherwise).  Returns 0 on success, 1 on failure (message
+ * in the log, on stderr and in gfb_last_error), like run_forward.
  */
 int32_t gfb_run_forward(const char* direction, int32_t resume, int32_t effective_nprocs);
+
+/*
+ * The partition merge of gfb_run_forward on its own, for checking and for
+ * merging once ahead of runs: reads partition_dir/partition_{r}.<extension>
+ * for r = 0, 1, ... and writes the merged set (read_partition_all,
+ * io.cpp:319-450) to out_path (.gfr or .h5): attributes n_partitions,
+ * n_cell, ngll, n_rank_node; datasets local_cell_ids, local_cell2rank_node
+ * [n_cell, ngll^3] (the concatenated local_cell2global_node), the per-point
+ * fields, pml_region and recording/{gll_node_ids, gll_node_coords,
+ * rec_cell_local, rec_cell_global_ids, cell_gll_node_index}.  Needs no GPU.
+ */
+gfb_status gfb_merge_partitions(const char* partition_dir, const char* extension, const char* out_path);
+
+/* Number of CUDA devices visible to the process (0 when there is none or the
+ * driver cannot be reached); main.cpp:43-58 exits 1 when it is 0. */
+gfb_status gfb_device_count(int32_t* n);
 
 #ifdef __cplusplus
 }
