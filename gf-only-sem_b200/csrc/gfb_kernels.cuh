@@ -57,6 +57,25 @@ struct ModelConst {
     double dt, half_dt2, c1, c2;
 };
 constexpr int kMaxModels = 255;
+// Wavefields one solver advances together: force directions times source
+// positions (a source set per position, each with its cells, weights and
+// source time function).
+constexpr int kMaxFields = 12;
+
+// Direction and source set of wavefield f (kernel parameters are indexed
+// with compile-time indices only).
+template <int NFLD>
+__device__ __forceinline__ void field_source(const int (&dir)[kMaxFields], const int (&fset)[kMaxFields], int f,
+                                             int& d, int& k) {
+    d = dir[0];
+    k = fset[0];
+#pragma unroll
+    for (int q = 1; q < NFLD; ++q)
+        if (f == q) {
+            d = dir[q];
+            k = fset[q];
+        }
+}
 
 template <int NG>
 struct Shape {
@@ -131,10 +150,13 @@ struct ElemArgs {
     const int* src_head;  // [cell] first source slot or -1
     const int* src_next;  // [slot]
     const Real* src_w;    // [slot][NN]
-    const Real* mstf;     // [model] source time function value of this step (nullptr: none)
+    const Real* mstf;     // [model][set] source time function value of this step (nullptr: none)
+    const int* src_set;   // [slot] source set of the slot (nullptr: every slot is set 0)
+    int n_set;            // source sets (one per source position)
     const int* mlive;     // [model] 1 while the model still steps
     const ModelConst* mc; // [model]
-    int dir0, dir1, dir2;
+    int dir[kMaxFields];  // force direction of each wavefield
+    int fset[kMaxFields]; // source set of each wavefield
     // finalisation of the nodes whose last touching colour this is (the
     // node update fused into the element kernel); fuse == 0 keeps the
     // force in memory for a separate node pass
@@ -277,20 +299,22 @@ __device__ __forceinline__ void elem_body(const ElemArgs<Real>& A, Real* smem) {
             prev[f * NN] = nv;
         }
     }
-    // point-force source
-    const Real stf = A.mstf ? A.mstf[0] : Real(0);
-    if (stf != Real(0)) {
+    // point-force source (one model): wavefield d takes the slots of its
+    // source set, scaled by that set's source time function
+    if (A.mstf) {
         int s = A.src_head ? __ldg(A.src_head + e) : -1;
         while (s >= 0) {
             const Real w = __ldg(A.src_w + (size_t)s * NN + p);
+            const int ks = A.src_set ? __ldg(A.src_set + s) : 0;
             if (w != Real(0)) {
-                const Real sw = stf * w;
-                const int dirs[3] = {A.dir0, A.dir1, A.dir2};
 #pragma unroll
-                for (int d = 0; d < NFLD; ++d)
+                for (int d = 0; d < NFLD; ++d) {
+                    const Real stf = A.mstf[A.fset[d]];
+                    if (stf == Real(0) || A.fset[d] != ks) continue;
 #pragma unroll
                     for (int c = 0; c < 3; ++c)
-                        if (c == dirs[d]) r[d * 3 + c] += sw;
+                        if (c == A.dir[d]) r[d * 3 + c] += stf * w;
+                }
             }
             s = __ldg(A.src_next + s);
         }
@@ -480,15 +504,19 @@ __global__ void __launch_bounds__(256, 2) node_pml_kernel(NodeArgs<Real> A, Node
 // the end of the series inject nothing).  mstep[m] is the step about to be
 // computed and moves on by one while the model steps, so a captured step
 // replays correctly.
+// Series q = m * n_set + k is source set k of model m.
 template <typename Real>
-__global__ void step_begin_kernel(int n_model, int* mstep, const int* nsteps, const int* n_stf,
+__global__ void step_begin_kernel(int n_model, int n_set, int* mstep, const int* nsteps, const int* n_stf,
                                   const long long* stf_off, const Real* stf_all, Real* mstf, int* mlive) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n_model) return;
     const int t = mstep[m];
     const bool live = t < nsteps[m];
     mlive[m] = live ? 1 : 0;
-    mstf[m] = (live && t < n_stf[m]) ? stf_all[stf_off[m] + t] : Real(0);
+    for (int k = 0; k < n_set; ++k) {
+        const int q = m * n_set + k;
+        mstf[q] = (live && t < n_stf[q]) ? stf_all[stf_off[q] + t] : Real(0);
+    }
     mstep[m] = t + (live ? 1 : 0);
 }
 
@@ -778,20 +806,21 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
                     }
                 }
             }
-            // point force (solver.cpp:577-605)
-            const Real stf = A.mstf ? __ldg(A.mstf + mdl) : Real(0);
-            if (stf != Real(0)) {
+            // point force (solver.cpp:577-605): wavefield d takes the slots
+            // of its source set, scaled by that set's source time function
+            if (A.mstf) {
                 int s = A.src_head ? __ldg(A.src_head + e) : -1;
                 while (s >= 0) {
                     const Real w = __ldg(A.src_w + (size_t)s * NN + p);
+                    const int ks = A.src_set ? __ldg(A.src_set + s) : 0;
                     if (w != Real(0)) {
-                        const Real sw = stf * w;
 #pragma unroll
                         for (int d = 0; d < NFLD; ++d) {
-                            const int dir = (d == 0) ? A.dir0 : ((d == 1) ? A.dir1 : A.dir2);
+                            const Real stf = __ldg(A.mstf + mdl * A.n_set + A.fset[d]);
+                            if (stf == Real(0) || A.fset[d] != ks) continue;
 #pragma unroll
                             for (int c = 0; c < 3; ++c)
-                                if (c == dir) r[d][c] += sw;
+                                if (c == A.dir[d]) r[d][c] += stf * w;
                         }
                     }
                     s = __ldg(A.src_next + s);
@@ -887,10 +916,13 @@ struct ColArgs {
     const int* src_head;
     const int* src_next;
     const float* src_w;
-    const float* mstf;             // [model] source time function value of this step
+    const float* mstf;             // [model][set] source time function value of this step
+    const int* src_set;            // [slot] source set (nullptr: all set 0)
+    int n_set;                     // n_model * n_set <= kMaxModels
     const int* mlive;              // [model] 1 while the model still steps
     int n_model;                   // <= kMaxModels
-    int dir[3];
+    int dir[kMaxFields];
+    int fset[kMaxFields];
     float D[36];                   // D[i*NG+s], read with compile-time indices only
 };
 
@@ -917,14 +949,13 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     const int col = lane_ok ? tid - line * NG2 : 0;
     const int cl = line / NFLD, fld = line - cl * NFLD;
     const int j = col / NG, k = col - j * NG;
-    const int dir = fld == 0 ? A.dir[0] : (fld == 1 ? A.dir[1] : A.dir[2]);
+    int dir, fs;
+    field_source<NFLD>(A.dir, A.fset, fld, dir, fs);
     // per-model step flags and source values of this step, read once per block
     __shared__ float s_stf[kMaxModels];
     __shared__ int s_live[kMaxModels];
-    for (int m = tid; m < A.n_model; m += S::THREADS) {
-        s_stf[m] = A.mstf[m];
-        s_live[m] = A.mlive[m];
-    }
+    for (int m = tid; m < A.n_model * A.n_set; m += S::THREADS) s_stf[m] = A.mstf[m];
+    for (int m = tid; m < A.n_model; m += S::THREADS) s_live[m] = A.mlive[m];
     if (tid < NG2) sD[tid] = A.dmat[tid];
     __syncthreads();
     float Dj[NG], Dk[NG], Tj[NG], Tk[NG];
@@ -1030,7 +1061,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(pf));
                 }
         }
-        const float stf = act ? s_stf[mdl] : 0.f;
+        const float stf = act ? s_stf[mdl * A.n_set + fs] : 0.f;
         const int src = (act && stf != 0.f && A.src_head) ? __ldg(A.src_head + e) : -1;
         pre_ok = line_nodes(nx, (it + 1) % 3, nw);
         load_vectors(nw, pre_ok, pre);
@@ -1128,6 +1159,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                 r[2] = -r[2];
                 // point force (solver.cpp:577-605)
                 for (int sl = src; sl >= 0; sl = __ldg(A.src_next + sl)) {
+                    if (A.src_set && __ldg(A.src_set + sl) != fs) continue;
                     const float w = __ldg(A.src_w + (size_t)sl * NN + p);
                     if (w != 0.f) {
                         const float sw = stf * w;

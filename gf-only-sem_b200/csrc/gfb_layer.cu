@@ -795,6 +795,7 @@ gfb_status gfb_layer_attach(gfb_solver* s, const gfb_layer* layer, const uint16_
     if (!s || !layer || !weights || !scales) return set_error(GFB_ERR_INVALID, "NULL argument");
     const SolverView v = solver_view(s);
     if (v.precision != GFB_FP32) return set_error(GFB_ERR_UNSUPPORTED, "the learned layer runs on the FP32 path");
+    if (v.n_field > 3) return set_error(GFB_ERR_UNSUPPORTED, "the learned layer takes at most 3 wavefields");
     if (v.n_model != 1) return set_error(GFB_ERR_UNSUPPORTED, "the learned layer needs a single-model solver");
     LCU(cudaSetDevice(v.device));
     auto L = std::make_unique<Layer>();
@@ -905,7 +906,7 @@ gfb_status gfb_trainer_collect(gfb_trainer* t, gfb_solver* thin, gfb_solver* thi
     if (!t || !thin || !thick || !thin_to_thick || !layer) return set_error(GFB_ERR_INVALID, "NULL argument");
     if (n_steps < 0 || sample_stride < 1 || node_stride < 1) return set_error(GFB_ERR_INVALID, "trainer: bad strides");
     const SolverView a = solver_view(thin), b = solver_view(thick);
-    if (a.precision != GFB_FP32 || b.precision != GFB_FP32 || a.n_field != b.n_field || a.device != b.device ||
+    if (a.precision != GFB_FP32 || b.precision != GFB_FP32 || a.n_field != b.n_field || a.n_field > 3 || a.device != b.device ||
         a.device != t->device || a.n_model != 1 || b.n_model != 1)
         return set_error(GFB_ERR_INVALID, "trainer: thin and thick solvers must be single-model FP32 solvers with "
                                           "the same wavefields on the trainer's device");

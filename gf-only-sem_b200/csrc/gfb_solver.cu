@@ -19,6 +19,7 @@
 #include <string>
 #include <thread>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/gfb.h"
@@ -232,7 +233,12 @@ struct gfb_solver {
     int n_cell = 0, n_node = 0;
     double dt = 0.0;
     int stride = 0;
-    int dirs[3] = {0, 1, 2};
+    int dirs[gfb::kMaxFields] = {0, 1, 2};
+    int fset[gfb::kMaxFields] = {};    // source set of each wavefield
+    int n_set = 1;                     // source sets (positions), one model only when > 1
+    std::vector<gfb_source> sets;      // the sets during gfb_create (host arrays borrowed)
+    bool stf_from_sets = false;        // source time functions per set (else per model)
+    int* src_set = nullptr;            // [slot] set of each source slot (n_set > 1)
     int flags = 0;
     bool fuse = false;  // node update in the element kernel's last colour
     int step = 0;
@@ -527,11 +533,14 @@ gfb_status launch_elem_t(gfb_solver* s, int c) {
     A.src_next = s->src_next;
     A.src_w = static_cast<const Real*>(s->src_w);
     A.mstf = static_cast<const Real*>(s->d_mstf);
+    A.src_set = s->src_set;
+    A.n_set = s->n_set;
     A.mlive = s->d_mlive;
     A.mc = s->d_mc;
-    A.dir0 = s->dirs[0];
-    A.dir1 = s->dirs[1];
-    A.dir2 = s->dirs[2];
+    for (int d = 0; d < gfb::kMaxFields; ++d) {
+        A.dir[d] = s->dirs[d];
+        A.fset[d] = s->fset[d];
+    }
     A.fuse = s->fuse ? 1 : 0;
     node_args(s, A.nu, A.np);
     const int n = A.e_end - A.e_begin;
@@ -570,9 +579,14 @@ gfb_status launch_col_e(gfb_solver* s, int c) {
     A.src_next = s->src_next;
     A.src_w = static_cast<const float*>(s->src_w);
     A.mstf = static_cast<const float*>(s->d_mstf);
+    A.src_set = s->src_set;
+    A.n_set = s->n_set;
     A.mlive = s->d_mlive;
     A.n_model = s->n_model;
-    for (int d = 0; d < 3; ++d) A.dir[d] = s->dirs[d];
+    for (int d = 0; d < gfb::kMaxFields; ++d) {
+        A.dir[d] = s->dirs[d];
+        A.fset[d] = s->fset[d];
+    }
     for (int q = 0; q < 36; ++q) A.D[q] = q < NG * NG ? s->dmat_host[q] : 0.f;
     const int blocks = std::max(1, std::min(A.n_groups, s->col_blocks));
     gfb::elem_col_kernel<NG, NFLD, EPB><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
@@ -588,7 +602,9 @@ constexpr int col_epb_hi(int nfld) { return nfld == 3 ? 3 : (nfld == 2 ? 4 : 8);
 template <int NG, int NFLD>
 struct ColEpb {
     static constexpr int D = gfb::col_default_epb(NG, NFLD);
-    static constexpr int N = NG == 5 ? 3 : 1;
+    // the fewer / more cells-per-group variants exist for ngll 5 with up to
+    // three wavefields (more would exceed a block's threads)
+    static constexpr int N = (NG == 5 && NFLD <= 3) ? 3 : 1;
 };
 
 template <int NG, int NFLD>
@@ -689,6 +705,8 @@ gfb_status dispatch(int ng, int nfld, Args... args) {
     GFB_CASE(4, 1) GFB_CASE(4, 2) GFB_CASE(4, 3)
     GFB_CASE(5, 1) GFB_CASE(5, 2) GFB_CASE(5, 3)
     GFB_CASE(6, 1) GFB_CASE(6, 2) GFB_CASE(6, 3)
+    // several source positions: three directions each, at ngll 5
+    GFB_CASE(5, 6) GFB_CASE(5, 9) GFB_CASE(5, 12)
 #undef GFB_CASE
     return fail(GFB_ERR_UNSUPPORTED, "ngll=%d with %d wavefields is not supported", ng, nfld);
 }
@@ -808,9 +826,15 @@ gfb_status launch_node_f(gfb_solver* s) {
 
 template <typename Real>
 gfb_status launch_node_t(gfb_solver* s) {
-    if (s->nfld == 1) return launch_node_f<Real, 1>(s);
-    if (s->nfld == 2) return launch_node_f<Real, 2>(s);
-    return launch_node_f<Real, 3>(s);
+    switch (s->nfld) {
+        case 1: return launch_node_f<Real, 1>(s);
+        case 2: return launch_node_f<Real, 2>(s);
+        case 3: return launch_node_f<Real, 3>(s);
+        case 6: return launch_node_f<Real, 6>(s);
+        case 9: return launch_node_f<Real, 9>(s);
+        case 12: return launch_node_f<Real, 12>(s);
+        default: return fail(GFB_ERR_UNSUPPORTED, "%d wavefields in the node pass", s->nfld);
+    }
 }
 
 gfb_status launch_node(gfb_solver* s) {
@@ -1252,54 +1276,72 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         s->pml_prev = prev;
     }
     clk.mark("C-PML arrays");
-    // source: cells located by id (solver.cpp:250-258), chained per cell
-    if (src && src->n_src_cell > 0) {
-        std::vector<int> head(n_cell, -1), next(src->n_src_cell, -1), tail(n_cell, -1);
-        std::vector<Real> wts((size_t)src->n_src_cell * nn, Real(0));
-        int used = 0;
-        for (int si = 0; si < src->n_src_cell; ++si) {
-            long long found = -1;
-            for (long long e = 0; e < n_cell; ++e) {
-                const long long id = m->cell_ids ? m->cell_ids[e] : e;
-                if (id == src->cell_ids[si]) {
-                    found = e;
-                    break;
+    // source: cells located by id (solver.cpp:250-258), chained per cell;
+    // the slots of every source set (one per source position) in one list,
+    // each slot tagged with its set
+    {
+        long long n_slot = 0;
+        for (const auto& ss : s->sets) n_slot += std::max(0, ss.n_src_cell);
+        if (n_slot > 0) {
+            std::unordered_map<long long, long long> cell_of;
+            cell_of.reserve((size_t)n_cell * 2);
+            for (long long e = n_cell - 1; e >= 0; --e) cell_of[m->cell_ids ? m->cell_ids[e] : e] = e;
+            std::vector<int> head(n_cell, -1), next(n_slot, -1), tail(n_cell, -1), set_of(n_slot, 0);
+            std::vector<Real> wts((size_t)n_slot * nn, Real(0));
+            int used = 0;
+            long long si = 0;
+            for (int k = 0; k < (int)s->sets.size(); ++k) {
+                const gfb_source& ss = s->sets[k];
+                for (int q = 0; q < ss.n_src_cell; ++q, ++si) {
+                    set_of[si] = k;
+                    auto it = cell_of.find(ss.cell_ids[q]);  // the first cell with the id
+                    if (it == cell_of.end()) continue;       // not in this mesh (reference: -1, skipped)
+                    const int ed = inv_perm[it->second];
+                    for (int p = 0; p < nn; ++p) wts[(size_t)si * nn + p] = (Real)ss.weights[(size_t)q * nn + p];
+                    if (head[ed] < 0) head[ed] = (int)si;
+                    else next[tail[ed]] = (int)si;
+                    tail[ed] = (int)si;
+                    ++used;
                 }
             }
-            if (found < 0) continue;  // not in this mesh (reference: -1, skipped)
-            const int ed = inv_perm[found];
-            for (int p = 0; p < nn; ++p) wts[(size_t)si * nn + p] = (Real)src->weights[(size_t)si * nn + p];
-            if (head[ed] < 0) head[ed] = si;
-            else next[tail[ed]] = si;
-            tail[ed] = si;
-            ++used;
+            s->has_src = used > 0;
+            s->n_src = (int)n_slot;
+            int *dh = nullptr, *dn = nullptr;
+            if ((st = s->alloc(&dh, head.size()))) return st;
+            if ((st = s->alloc(&dn, next.size()))) return st;
+            if ((st = h2d(s, dh, head.data(), head.size() * 4))) return st;
+            if ((st = h2d(s, dn, next.data(), next.size() * 4))) return st;
+            s->src_head = dh;
+            s->src_next = dn;
+            if ((st = upload(s, &s->src_w, wts))) return st;
+            if (s->n_set > 1) {
+                if ((st = s->alloc(&s->src_set, set_of.size()))) return st;
+                if ((st = h2d(s, s->src_set, set_of.data(), set_of.size() * 4))) return st;
+            }
         }
-        s->has_src = used > 0;
-        s->n_src = src->n_src_cell;
-        int *dh = nullptr, *dn = nullptr;
-        if ((st = s->alloc(&dh, head.size()))) return st;
-        if ((st = s->alloc(&dn, next.size()))) return st;
-        if ((st = h2d(s, dh, head.data(), head.size() * 4))) return st;
-        if ((st = h2d(s, dn, next.data(), next.size() * 4))) return st;
-        s->src_head = dh;
-        s->src_next = dn;
-        if ((st = upload(s, &s->src_w, wts))) return st;
     }
     clk.mark("source");
     // models: constants, step counters, source time functions
     {
+        // source time function series: one per model, or one per source
+        // set of the single model (series q = model * n_set + set)
+        const int n_series = n_model * s->n_set;
         std::vector<gfb::ModelConst> mc(n_model);
-        std::vector<int> nsteps(n_model), nstf(n_model), zero(n_model, 0), one(n_model, 1);
-        std::vector<long long> off(n_model);
-        std::vector<Real> stf_all, mstf(n_model, Real(0));
+        std::vector<int> nsteps(n_model), nstf(n_series), zero(n_model, 0), one(n_model, 1);
+        std::vector<long long> off(n_series);
+        std::vector<Real> stf_all, mstf(n_series, Real(0));
         const double theta = 1.0 / 8.0;  // pml.cpp:35, 63-64
         for (int k = 0; k < n_model; ++k) {
             const double dt = models[k].dt;
             mc[k] = gfb::ModelConst{dt, 0.5 * dt * dt, (1.0 - 2.0 * theta) * 0.5 * dt, (1.0 - theta) * 0.5 * dt * dt};
             nsteps[k] = models[k].n_steps;
-            nstf[k] = std::max(0, models[k].n_stf);
-            off[k] = (long long)stf_all.size();
-            for (int t = 0; t < nstf[k]; ++t) stf_all.push_back((Real)models[k].stf[t]);
+        }
+        for (int q = 0; q < n_series; ++q) {
+            const int n = s->stf_from_sets ? s->sets[q].n_stf : models[q].n_stf;
+            const double* v = s->stf_from_sets ? s->sets[q].stf : models[q].stf;
+            nstf[q] = std::max(0, n);
+            off[q] = (long long)stf_all.size();
+            for (int t = 0; t < nstf[q]; ++t) stf_all.push_back((Real)v[t]);
         }
         s->model_nsteps = nsteps;
         if (stf_all.empty()) stf_all.push_back(Real(0));
@@ -1422,7 +1464,7 @@ gfb_status launch_step_begin_t(gfb_solver* s) {
     const int threads = 128;
     const int blocks = (s->n_model + threads - 1) / threads;
     gfb::step_begin_kernel<Real><<<blocks, threads, 0, s->stream>>>(
-        s->n_model, s->d_mstep, s->d_nsteps, s->d_nstf, s->d_stf_off, static_cast<const Real*>(s->d_stf_all),
+        s->n_model, s->n_set, s->d_mstep, s->d_nsteps, s->d_nstf, s->d_stf_off, static_cast<const Real*>(s->d_stf_all),
         static_cast<Real*>(s->d_mstf), s->d_mlive);
     CU(cudaGetLastError());
     s->launches++;
@@ -1614,11 +1656,22 @@ bool greedy_colour(const gfb_mesh* m, int nn, std::vector<T>& used, std::vector<
     return true;
 }
 
+// Wavefields of a solver with several source positions: count, force
+// direction and source set of each, and the sets.
+struct FieldSpec {
+    int n_field = 0;
+    int dir[gfb::kMaxFields] = {};
+    int fset[gfb::kMaxFields] = {};
+    int n_set = 0;
+    const gfb_source* sets = nullptr;
+};
+
 // w_tab / D_tab: GLL weights [ngll] and derivative matrix [ngll*ngll] to use
-// instead of the tables computed from ngll (NULL: computed).
+// instead of the tables computed from ngll (NULL: computed).  fs: the
+// wavefields and source sets (NULL: config's wavefields, all with src).
 gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, int n_model,
                        const gfb_model* models, gfb_solver** out, const double* w_tab = nullptr,
-                       const double* D_tab = nullptr) {
+                       const double* D_tab = nullptr, const FieldSpec* fs = nullptr) {
     gfb_status st;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -1631,13 +1684,20 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     s->prec = c->precision;
     s->ng = m->ngll;
     s->nn = m->ngll * m->ngll * m->ngll;
-    s->nfld = c->n_field;
-    s->F = 3 * c->n_field;
+    s->nfld = fs ? fs->n_field : c->n_field;
+    s->F = 3 * s->nfld;
     s->n_cell = m->n_cell;
     s->n_node = m->n_node;
     s->dt = c->dt;
     s->stride = c->snapshot_stride;
-    for (int d = 0; d < 3; ++d) s->dirs[d] = d < c->n_field ? c->field_dir[d] : 0;
+    for (int d = 0; d < gfb::kMaxFields; ++d) {
+        s->dirs[d] = fs ? fs->dir[d] : (d < c->n_field ? c->field_dir[d] : 0);
+        s->fset[d] = fs ? fs->fset[d] : 0;
+    }
+    s->n_set = fs ? fs->n_set : 1;
+    s->stf_from_sets = fs != nullptr;
+    if (fs) s->sets.assign(fs->sets, fs->sets + fs->n_set);
+    else if (src) s->sets.assign(1, *src);
     s->has_cpml = m->pml_coef_abar != nullptr;
     s->flags = c->flags;
     s->rec_f32 = (c->flags & GFB_FLAG_RECORD_F32) != 0;
@@ -1801,6 +1861,7 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     if ((c->flags & GFB_FLAG_AUTOTUNE) && (st = autotune(s.get()))) return st;
     CU(cudaDeviceSynchronize());
     clk.mark("autotune");
+    s->sets.clear();  // the caller's source arrays were borrowed for the call
     *out = s.release();
     return GFB_OK;
 }
@@ -1824,6 +1885,51 @@ gfb_status gfb_create(const gfb_mesh* m, const gfb_config* c, const gfb_source* 
     one.n_stf = src ? src->n_stf : 0;
     one.stf = src ? src->stf : nullptr;
     return create_impl(m, c, src, 1, &one, out);
+}
+
+gfb_status gfb_create_sources(const gfb_mesh* m, const gfb_config* c, int32_t n_source, const gfb_source* sources,
+                              int32_t n_field, const int32_t* field_dir, const int32_t* field_source,
+                              gfb_solver** out) {
+    if (!out) return fail(GFB_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!m || !c) return fail(GFB_ERR_INVALID, "mesh and config are required");
+    if (n_source < 1 || n_source > gfb::kMaxFields || !sources)
+        return fail(GFB_ERR_INVALID, "n_source must be 1..%d", gfb::kMaxFields);
+    if (!field_dir || !field_source) return fail(GFB_ERR_INVALID, "field_dir and field_source are required");
+    const bool shape_ok = (n_field >= 1 && n_field <= 3) || (m->ngll == 5 && (n_field == 6 || n_field == 9 || n_field == 12));
+    if (!shape_ok)
+        return fail(GFB_ERR_UNSUPPORTED, "%d wavefields: 1..3 at any ngll, or 6, 9, 12 at ngll 5", n_field);
+    if (c->precision == GFB_FP64 && n_field > 6)
+        return fail(GFB_ERR_UNSUPPORTED, "the FP64 path advances at most 6 wavefields (%d asked)", n_field);
+    FieldSpec fs;
+    fs.n_field = n_field;
+    fs.n_set = n_source;
+    fs.sets = sources;
+    for (int f = 0; f < n_field; ++f) {
+        if (field_dir[f] < 0 || field_dir[f] > 2)
+            return fail(GFB_ERR_INVALID, "field_dir[%d]=%d must be 0, 1 or 2", f, field_dir[f]);
+        if (field_source[f] < 0 || field_source[f] >= n_source)
+            return fail(GFB_ERR_INVALID, "field_source[%d]=%d must be 0..%d", f, field_source[f], n_source - 1);
+        fs.dir[f] = field_dir[f];
+        fs.fset[f] = field_source[f];
+    }
+    for (int k = 0; k < n_source; ++k) {
+        const gfb_source& ss = sources[k];
+        if (ss.n_src_cell < 0 || (ss.n_src_cell > 0 && (!ss.cell_ids || !ss.weights)) || ss.n_stf < 0 ||
+            (ss.n_stf > 0 && !ss.stf))
+            return fail(GFB_ERR_INVALID, "source %d: bad cells, weights or source time function", k);
+    }
+    gfb_config cc = *c;
+    cc.n_field = 1;  // the wavefields are those of field_dir / field_source
+    cc.field_dir[0] = 0;
+    gfb_status st = validate(m, &cc);
+    if (st) return st;
+    gfb_model one{};
+    one.cell_end = m->n_cell;
+    one.node_end = m->n_node;
+    one.dt = c->dt;
+    one.n_steps = INT32_MAX;
+    return create_impl(m, c, nullptr, 1, &one, out, nullptr, nullptr, &fs);
 }
 
 gfb_status gfb_create_batch(const gfb_mesh* m, const gfb_config* c, const gfb_source* src, int32_t n_model,

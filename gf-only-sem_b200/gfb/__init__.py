@@ -145,6 +145,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.gfb_checkpoint_load.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     lib.gfb_create_batch.argtypes = [C.POINTER(Mesh), C.POINTER(Config), C.POINTER(Source), C.c_int32,
                                      C.POINTER(Model), C.POINTER(C.c_void_p)]
+    lib.gfb_create_sources.argtypes = [C.POINTER(Mesh), C.POINTER(Config), C.c_int32, C.POINTER(Source), C.c_int32,
+                                       _ip, _ip, C.POINTER(C.c_void_p)]
     lib.gfb_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
     lib.gfb_current_step.argtypes = [C.c_void_p, _ip]
     lib.gfb_get_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
@@ -161,7 +163,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "gfb_get_state", "gfb_set_state", "gfb_records_pending", "gfb_read_record",
         "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
         "gfb_create_batch", "gfb_checkpoint_size", "gfb_checkpoint_save", "gfb_checkpoint_load",
-        "gfb_rec_nodes", "gfb_read_green", "gfb_read_record_f32",
+        "gfb_rec_nodes", "gfb_read_green", "gfb_read_record_f32", "gfb_create_sources",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -204,7 +206,11 @@ class Solver:
 
     def __init__(self, prob: dict, dirs: Sequence[int] = (0,), precision: int = FP64,
                  device: int = 0, record_slots: int = 4, record: bool = True, flags: int = 0,
-                 models: Optional[Sequence[dict]] = None):
+                 models: Optional[Sequence[dict]] = None, sources: Optional[Sequence[dict]] = None,
+                 field_source: Optional[Sequence[int]] = None):
+        """``sources`` (several source positions, gfb_create_sources): dicts
+        with src_cell_ids, src_weights and stf; wavefield f is driven by
+        sources[field_source[f]] in direction dirs[f]."""
         self.lib = load_library()
         keep = {}
 
@@ -246,7 +252,7 @@ class Solver:
         self.stride = c.snapshot_stride
         c.precision = int(precision)
         c.n_field = len(dirs)
-        for i, d in enumerate(dirs):
+        for i, d in enumerate(dirs[:3]):
             c.field_dir[i] = int(d)
         c.device = int(device)
         c.record_slots = int(record_slots)
@@ -260,7 +266,28 @@ class Solver:
         s.n_stf = 0 if stf is None else int(stf.size)
         s.stf = _ptr(stf, C.c_double)
         h = C.c_void_p()
-        if models is None:
+        if sources is not None:
+            if field_source is None or len(field_source) != len(dirs):
+                raise ValueError("field_source must give the source of every wavefield")
+            c.n_field = 1
+            c.field_dir[0] = 0
+            ss = (Source * len(sources))()
+            for k, d in enumerate(sources):
+                ids = np.ascontiguousarray(d["src_cell_ids"], dtype=np.int64).ravel()
+                w = np.ascontiguousarray(d["src_weights"], dtype=np.float64).ravel()
+                st = np.ascontiguousarray(d["stf"], dtype=np.float64).ravel()
+                keep[f"sids{k}"], keep[f"sw{k}"], keep[f"sstf{k}"] = ids, w, st
+                ss[k].n_src_cell = int(ids.size)
+                ss[k].cell_ids = _ptr(ids, C.c_int64)
+                ss[k].weights = _ptr(w, C.c_double)
+                ss[k].n_stf = int(st.size)
+                ss[k].stf = _ptr(st, C.c_double)
+            fd = np.ascontiguousarray(dirs, dtype=np.int32)
+            fsrc = np.ascontiguousarray(field_source, dtype=np.int32)
+            keep["fd"], keep["fsrc"] = fd, fsrc
+            _check(self.lib.gfb_create_sources(C.byref(m), C.byref(c), len(sources), ss, len(dirs),
+                                               _ptr(fd, C.c_int32), _ptr(fsrc, C.c_int32), C.byref(h)))
+        elif models is None:
             _check(self.lib.gfb_create(C.byref(m), C.byref(c), C.byref(s), C.byref(h)))
         else:
             md = (Model * len(models))()

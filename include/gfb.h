@@ -175,6 +175,22 @@ typedef struct gfb_model {
 gfb_status gfb_create_batch(const gfb_mesh* mesh, const gfb_config* config, const gfb_source* source,
                             int32_t n_model, const gfb_model* models, gfb_solver** out);
 
+/*
+ * One solver for several source positions (no counterpart in the
+ * reference, which runs one source and one direction per process): the
+ * geometry and materials are read once per step for all wavefields.
+ * sources[0..n_source) are point sources as gfb_source (cells, weights,
+ * stf); wavefield f is driven by source field_source[f] in direction
+ * field_dir[f] (0=x 1=y 2=z).  n_field: 1..3 at any ngll, or 6, 9 or 12 at
+ * ngll 5 (two to four positions times x/y/z); the FP64 path takes at most 6.
+ * config->n_field and config->field_dir are not used.  Records, state and
+ * Green's functions are per wavefield as for gfb_create.
+ */
+#define GFB_MAX_FIELDS 12
+gfb_status gfb_create_sources(const gfb_mesh* mesh, const gfb_config* config, int32_t n_source,
+                              const gfb_source* sources, int32_t n_field, const int32_t* field_dir,
+                              const int32_t* field_source, gfb_solver** out);
+
 /* Release all device and host memory.  Replaces cuda_free_state
  * (cuda_step.hpp:80-81). */
 gfb_status gfb_destroy(gfb_solver* solver);

@@ -355,3 +355,48 @@ def test_resume_from_state_matches_uninterrupted_run():
     second.advance(50)
     for x, y in zip(second.state(0), full.state(0)):
         np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-12 * np.abs(y).max())
+
+
+def two_positions():
+    """The layered 6 x 5 x 4 problem with a second point force at another
+    position (its own cells, weights and a Ricker of another frequency)."""
+    prob = layered_problem(nsteps=120)
+    other = layered_problem(nsteps=120)
+    spec = other["spec"]
+    src2 = mesh.locate_point_source(other["coords"], mesh.cell_corners(spec, mesh.vertex_grid(spec)),
+                                    np.array([2150.0, 1020.0, 880.0]), other["is_pml"], spec.order)
+    s2 = {"src_cell_ids": src2[0], "src_weights": src2[1],
+          "stf": mesh.ricker(np.arange(120) * prob["dt"], f0=2.7, t0=0.8)}
+    s1 = {k: prob[k] for k in ("src_cell_ids", "src_weights", "stf")}
+    return prob, [s1, s2]
+
+
+@pytest.mark.parametrize("prec,tol", [(gfb.FP64, FP64_TOL), (gfb.FP32, FP32_TOL)])
+def test_two_source_positions_times_three_directions_in_one_solver(prec, tol):
+    """2 positions x 3 directions = 6 wavefields in one launch per colour
+    (gfb_create_sources); each wavefield equals the oracle run of its own
+    source and direction."""
+    prob, sources = two_positions()
+    dirs, fsrc = [0, 1, 2, 0, 1, 2], [0, 0, 0, 1, 1, 1]
+    s = gfb.Solver(prob, dirs=dirs, precision=prec, sources=sources, field_source=fsrc)
+    assert s.info()["n_field"] == 6
+    s.advance(120)
+    snaps = s.drain()
+    for f, (d, k) in enumerate(zip(dirs, fsrc)):
+        p = dict(prob, **sources[k])
+        ref, (u, v, a) = oracle_snaps(p, d, 120)
+        for q in ("strain", "u", "v"):
+            e = rel_l2(snaps[f][q], ref[q])
+            assert e <= tol, (f, q, e)
+        if prec == gfb.FP64:
+            compare_runs(snaps[f], ref, tol, f"field {f}")
+            gu, gv, ga = s.state(f)
+            assert rel_l2(gu, u) <= tol and rel_l2(gv, v) <= tol
+
+
+def test_source_sets_are_checked():
+    prob, sources = two_positions()
+    with pytest.raises(gfb.GfbError):
+        gfb.Solver(prob, dirs=[0, 1, 2, 0], precision=gfb.FP32, sources=sources, field_source=[0, 0, 0, 1])
+    with pytest.raises(gfb.GfbError):
+        gfb.Solver(prob, dirs=[0, 1], precision=gfb.FP32, sources=sources, field_source=[0, 2])
