@@ -419,15 +419,20 @@ def node_pml_live_axes(prob):
 def elem_bytes_per_step(prob, info, n_field, prec):
     """Algorithmic DRAM bytes of one step's element/assembly launches
     (unpadded component bytes; the [node][field][4] layout moves 4/3 of the
-    gather/force bytes, visible in the ncu traffic)."""
+    gather/force bytes, visible in the ncu traffic).  With the force updated
+    by increments (99 of 100 steps) every touch of a node reads and writes
+    its force."""
     nn = 125
     P = prob["n_cell"] * nn
     G = prob["n_node"]
     sr = 4 if prec == 1 else 8
     F = 3 * n_field
     geom = P * 12 * sr + P * 4                      # geometry + ibool
-    gather = P * F * sr                              # predicted displacement
-    force = G * F * sr + (P - G) * F * sr * 2        # first touch writes, others read+write
+    gather = P * F * sr                              # predicted displacement (or its increment)
+    if info.get("force_refresh", 1) > 1:             # force by increments: every touch reads and writes
+        force = P * F * sr * 2
+    else:                                            # in full: first touch writes, others read+write
+        force = G * F * sr + (P - G) * F * sr * 2
     pml = 0
     if info["n_pml_node"] == 0:                      # per-cell C-PML in this kernel
         Ppml = info["n_pml_cell"] * nn
@@ -436,12 +441,22 @@ def elem_bytes_per_step(prob, info, n_field, prec):
 
 
 def node_bytes_per_step(prob, info, n_field, prec):
+    """Algorithmic DRAM bytes of one step's node passes: per node and value
+    u and v read and written (FP64), the acceleration read and written
+    (Real; not at plain nodes in the half-step velocity form), the assembled
+    force read and the next predicted displacement (or its increment)
+    written (Real, unpadded), the mass (1/m in FP32); plus the node-form
+    C-PML coefficients, previous field and memory of the live axes."""
     sr = 4 if prec == 1 else 8
     F = 3 * n_field
-    base = prob["n_node"] * (F * (32 + 2 * sr + sr + sr) + 8 + (4 if prec == 1 else 0))
-    if info["n_pml_node"] > 0:                       # node-form C-PML in this kernel
-        n_pml, live = node_pml_live_axes(prob)
-        base += n_pml * (4 + 14 * sr + F * sr * 2) + live * F * sr * 2
+    n_pml = info["n_pml_node"]
+    n_plain = prob["n_node"] - n_pml
+    acc = 0 if info.get("half_v") else 2 * sr
+    mass = 4 if prec == 1 else 8
+    base = n_plain * (F * (32 + acc + 2 * sr) + mass) + n_pml * (F * (32 + 4 * sr) + mass)
+    if n_pml > 0:                                    # node-form C-PML in this kernel
+        n_live, live = node_pml_live_axes(prob)
+        base += n_live * (14 * sr + F * sr * 2) + live * F * sr * 2
     return base
 
 

@@ -43,6 +43,11 @@ SolverView solver_view(gfb_solver* s);
 // (after u, v, a were written from outside the time loop).
 gfb_status solver_predict(gfb_solver* s);
 
+// Keep (u, v, a) at every node from now on (the FP32 path otherwise holds
+// the half-step velocity and no acceleration at its plain nodes); for code
+// that reads or writes v and a of any node between steps.
+gfb_status solver_full_state(gfb_solver* s);
+
 // Learned absorbing layer attached to a solver (gfb_layer.cu): launched
 // between the element phase and the node phase of every step; freed with the
 // solver.

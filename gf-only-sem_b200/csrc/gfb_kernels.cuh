@@ -102,6 +102,14 @@ struct NodeArgs {
     const ModelConst* mc;
     const int* mlive;
     const long long* live_node_end;  // [2] end of the stepping C-PML / plain nodes (several models), or null
+    // [model] 1 when the model's next step evaluates the element force in
+    // full (the node pass then stores the predicted displacement), 0 when
+    // it adds the force of the step's increment (the node pass stores the
+    // increment of the predicted displacement); nullptr: always in full
+    const int* mnext;
+    // plain nodes keep the half-step velocity v + dt/2 a in v and no
+    // acceleration (see update_node_field)
+    bool half_v;
 };
 
 // C-PML at global nodes (FP32 path).
@@ -154,6 +162,8 @@ struct ElemArgs {
     const int* src_set;   // [slot] source set of the slot (nullptr: every slot is set 0)
     int n_set;            // source sets (one per source position)
     const int* mlive;     // [model] 1 while the model still steps
+    const int* mdirect;   // [model] 1: this step evaluates the force in full (first touch stores), 0: adds the
+                          // increment's force to the stored one; nullptr: in full
     const ModelConst* mc; // [model]
     int dir[kMaxFields];  // force direction of each wavefield
     int fset[kMaxFields]; // source set of each wavefield
@@ -367,6 +377,13 @@ __device__ __forceinline__ void store4(double* p, double a, double b, double c, 
     reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
 }
 
+// FP64 operations rounded one by one (no contraction into FMA), so that the
+// node update rounds the same way in every instantiation of the kernels
+// that inline it (a solver of one model and of several must agree bit for
+// bit) and in the reference's evaluation order.
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+
 // Finalise wavefield d of node g from its complete assembled force fv:
 // node C-PML term (when PML), Newmark corrector with the diagonal mass
 // (solver.cpp:52-69, legacy damping of 564-574 applied to v first) and the
@@ -376,12 +393,43 @@ __device__ __forceinline__ void store4(double* p, double a, double b, double c, 
 // stores 0 there), so the f64 mass is not read.
 template <typename Real, int NFLD, bool PML>
 __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const NodePml<Real>& P, long long g,
-                                                  int d, const Real (&fv)[3], int sl, const ModelConst& K) {
+                                                  int d, const Real (&fv)[3], int sl, const ModelConst& K,
+                                                  bool full = true) {
     constexpr int F = 3 * NFLD;
     const long long i0 = g * F + d * 3;
     double* __restrict__ pu = A.u + i0;
     double* __restrict__ pv = A.v + i0;
     Real* __restrict__ pa = A.a + i0;
+    if (!PML && A.half_v) {
+        // Newmark with beta = 0, gamma = 1/2 (solver.cpp:40-69) written on
+        // the half-step velocity w = v + dt/2 a: u_{n+1} = u_n + dt w_n,
+        // a_{n+1} = f/m, w_{n+1} = w_n + dt a_{n+1}, and the next predicted
+        // displacement u_{n+1} + dt w_{n+1} (its increment dt w_{n+1}).  The
+        // same values as the (u, v, a) form in exact arithmetic, without the
+        // acceleration's read and write; v and a are recovered from w and
+        // the assembled force when they are needed (records, state).
+        double uu[3], ww[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            uu[c] = pu[c];
+            ww[c] = pv[c];
+        }
+        const Real im = __ldg(A.inv_mass + g);
+        Real out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (im != Real(0)) {  // m <= 0: the node stays as it is (a = 0, solver.cpp:58-61)
+                const double a_new = (double)(Real)(fv[c] * im);
+                uu[c] = dadd(uu[c], dmul(K.dt, ww[c]));
+                ww[c] = dadd(ww[c], dmul(K.dt, a_new));
+                pu[c] = uu[c];
+                pv[c] = ww[c];
+            }
+            out[c] = full ? (Real)dadd(uu[c], dmul(K.dt, ww[c])) : (Real)dmul(K.dt, ww[c]);
+        }
+        store4(A.ut + ((size_t)g * NFLD + d) * 4, out[0], out[1], out[2], Real(0));
+        return;
+    }
     double vv[3], uu[3];
     Real ao[3];
 #pragma unroll
@@ -411,10 +459,10 @@ __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const
     Real out[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        if (dmp > 0.0) vv[c] -= dmp * vv[c];
+        if (dmp > 0.0) vv[c] = __dsub_rn(vv[c], dmul(dmp, vv[c]));
         Real force = fv[c];
         if (PML && sl >= 0) {
-            const Real nv = (Real)(uu[c] + K.c1 * vv[c]);
+            const Real nv = (Real)dadd(uu[c], dmul(K.c1, vv[c]));
             const Real ov = pr[c] + (Real)K.c2 * ao[c];
             force += cf[0] * (Real)vv[c] + cf[1] * (Real)uu[c] + cf[2] * mm[0][c] + cf[3] * mm[1][c] + cf[4] * mm[2][c];
 #pragma unroll
@@ -428,16 +476,21 @@ __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const
         if (massless) {
             a_new = 0.0;
         } else {
-            a_new = A.inv_mass ? (double)(force * im) : (double)force / m;
+            a_new = A.inv_mass ? (double)(force * im) : __ddiv_rn((double)force, m);
             a_new = (double)(Real)a_new;
             const double a_old = (double)ao[c];
-            uu[c] += K.dt * vv[c] + K.dt * K.dt * ((0.5 - A.beta) * a_old + A.beta * a_new);
-            vv[c] += K.dt * ((1.0 - A.gamma) * a_old + A.gamma * a_new);
+            // solver.cpp:62-66
+            const double ta = dadd(dmul(0.5 - A.beta, a_old), dmul(A.beta, a_new));
+            uu[c] = dadd(uu[c], dadd(dmul(K.dt, vv[c]), dmul(dmul(K.dt, K.dt), ta)));
+            vv[c] = dadd(vv[c], dmul(K.dt, dadd(dmul(1.0 - A.gamma, a_old), dmul(A.gamma, a_new))));
         }
         pu[c] = uu[c];
         pv[c] = vv[c];
         pa[c] = (Real)a_new;
-        out[c] = (Real)(uu[c] + K.dt * vv[c] + K.half_dt2 * a_new);
+        // the next step's predicted displacement (solver.cpp:40-49), or its
+        // increment over this step's (u_{n+1} is this step's prediction)
+        const double inc = dadd(dmul(K.dt, vv[c]), dmul(K.half_dt2, a_new));
+        out[c] = full ? (Real)dadd(uu[c], inc) : (Real)inc;
     }
     store4(A.ut + ((size_t)g * NFLD + d) * 4, out[0], out[1], out[2], Real(0));
 }
@@ -453,14 +506,16 @@ __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const
 // taken all its steps (its state stays as it is).
 template <typename Real, bool MULTI>
 __device__ __forceinline__ bool node_constants(const NodeArgs<Real>& A, const NodePml<Real>& P, long long g,
-                                               ModelConst& K) {
+                                               ModelConst& K, bool& full) {
     if (!MULTI) {
         K = ModelConst{A.dt, A.half_dt2, P.c1, P.c2};
+        full = A.mnext ? A.mnext[0] != 0 : true;
         return true;
     }
     const int m = __ldg(A.node_model + g);
     if (!__ldg(A.mlive + m)) return false;
     K = A.mc[m];
+    full = A.mnext ? A.mnext[m] != 0 : true;
     return true;
 }
 
@@ -474,11 +529,12 @@ __global__ void __launch_bounds__(256, 3) node_update_kernel(NodeArgs<Real> A, N
         const int d = (int)(t - gl * NFLD);
         const long long g = g0 + gl;
         ModelConst K;
-        if (!node_constants<Real, MULTI>(A, P, g, K)) continue;
+        bool full;
+        if (!node_constants<Real, MULTI>(A, P, g, K, full)) continue;
         Real fv4[4];
         load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv4);
         const Real fv[3] = {fv4[0], fv4[1], fv4[2]};
-        update_node_field<Real, NFLD, false>(A, P, g, d, fv, -1, K);
+        update_node_field<Real, NFLD, false>(A, P, g, d, fv, -1, K, full);
     }
 }
 
@@ -491,11 +547,12 @@ __global__ void __launch_bounds__(256, 2) node_pml_kernel(NodeArgs<Real> A, Node
         const long long g = t / NFLD;
         const int d = (int)(t - g * NFLD);
         ModelConst K;
-        if (!node_constants<Real, MULTI>(A, P, g, K)) continue;
+        bool full;
+        if (!node_constants<Real, MULTI>(A, P, g, K, full)) continue;
         Real fv4[4];
         load4_nc(A.force + ((size_t)g * NFLD + d) * 4, fv4);
         const Real fv[3] = {fv4[0], fv4[1], fv4[2]};
-        update_node_field<Real, NFLD, true>(A, P, g, d, fv, (int)g, K);
+        update_node_field<Real, NFLD, true>(A, P, g, d, fv, (int)g, K, full);
     }
 }
 
@@ -505,17 +562,36 @@ __global__ void __launch_bounds__(256, 2) node_pml_kernel(NodeArgs<Real> A, Node
 // computed and moves on by one while the model steps, so a captured step
 // replays correctly.
 // Series q = m * n_set + k is source set k of model m.
+//
+// Element force in full or by increments: a step whose element phase
+// evaluates the force of the full predicted displacement (mdirect = 1: the
+// first colour touching a node stores) is followed by up to period-1 steps
+// that add the force of the predicted displacement's increment to the
+// stored force (mdirect = 0); the source then adds the increment of the
+// source time function.  A one-shot force_direct[m] (set by the host after
+// the predicted displacement was rewritten from u, v, a) makes the step a
+// full one.  mnext[m] tells the node pass what the next step needs.
 template <typename Real>
 __global__ void step_begin_kernel(int n_model, int n_set, int* mstep, const int* nsteps, const int* n_stf,
-                                  const long long* stf_off, const Real* stf_all, Real* mstf, int* mlive) {
+                                  const long long* stf_off, const Real* stf_all, Real* mstf, int* mlive, int period,
+                                  int* force_direct, int* mdirect, int* mnext) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n_model) return;
     const int t = mstep[m];
     const bool live = t < nsteps[m];
     mlive[m] = live ? 1 : 0;
+    bool full = true;
+    if (mdirect) {
+        full = period <= 1 || force_direct[m] != 0 || t % period == 0;
+        force_direct[m] = 0;
+        mdirect[m] = full ? 1 : 0;
+        mnext[m] = (period <= 1 || (t + 1) % period == 0) ? 1 : 0;
+    }
     for (int k = 0; k < n_set; ++k) {
         const int q = m * n_set + k;
-        mstf[q] = (live && t < n_stf[q]) ? stf_all[stf_off[q] + t] : Real(0);
+        const Real now = (live && t < n_stf[q]) ? stf_all[stf_off[q] + t] : Real(0);
+        const Real before = (!full && t >= 1 && t - 1 < n_stf[q]) ? stf_all[stf_off[q] + t - 1] : Real(0);
+        mstf[q] = full ? now : (live ? now - before : Real(0));
     }
     mstep[m] = t + (live ? 1 : 0);
 }
@@ -668,6 +744,7 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
         const int e = A.e_begin + grp * EPB + el;
         const int mdl = (e < A.e_end) ? (int)ib_of(ist, el)[NN] : 0;
         const bool active = (e < A.e_end) && (p < NN) && (!A.mlive || __ldg(A.mlive + mdl));
+        const uint32_t first_bit = (!A.mdirect || __ldg(A.mdirect + mdl)) ? kFirstTouch : 0u;
         Real* geo = geo_of(cur, el);
         Real* buf = buf_of(cur, el);
         uint32_t gword = 0;
@@ -681,7 +758,7 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
             mu = geo[11 * NN + p];
         }
         __syncthreads();  // geometry stage now takes this group's old force vectors
-        if (active && !(gword & kFirstTouch)) {
+        if (active && !(gword & first_bit)) {
             const uint32_t g = gword & kNodeMask;
 #pragma unroll
             for (int d = 0; d < NFLD; ++d)
@@ -831,7 +908,7 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
         __syncthreads();
         if (active) {
             const uint32_t g = gword & kNodeMask;
-            const bool first = gword & kFirstTouch;
+            const bool first = gword & first_bit;
             // the highest colour touching a node completes its force here and
             // finalises it: no cell reads the node later in this step
             const bool fin = A.fuse && (gword & kLastTouch);
@@ -920,6 +997,7 @@ struct ColArgs {
     const int* src_set;            // [slot] source set (nullptr: all set 0)
     int n_set;                     // n_model * n_set <= kMaxModels
     const int* mlive;              // [model] 1 while the model still steps
+    const int* mdirect;            // [model] 1: force in full this step, 0: by increment (nullptr: in full)
     int n_model;                   // <= kMaxModels
     int dir[kMaxFields];
     int fset[kMaxFields];
@@ -954,8 +1032,12 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     // per-model step flags and source values of this step, read once per block
     __shared__ float s_stf[kMaxModels];
     __shared__ int s_live[kMaxModels];
+    __shared__ int s_direct[kMaxModels];
     for (int m = tid; m < A.n_model * A.n_set; m += S::THREADS) s_stf[m] = A.mstf[m];
-    for (int m = tid; m < A.n_model; m += S::THREADS) s_live[m] = A.mlive[m];
+    for (int m = tid; m < A.n_model; m += S::THREADS) {
+        s_live[m] = A.mlive[m];
+        s_direct[m] = A.mdirect ? A.mdirect[m] : 1;
+    }
     if (tid < NG2) sD[tid] = A.dmat[tid];
     __syncthreads();
     float Dj[NG], Dk[NG], Tj[NG], Tk[NG];
@@ -1030,6 +1112,9 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         const int e = A.e_begin + grp * EPB + cl;
         const int mdl = pre_ok ? (int)ib_of(it % 3, cl)[NN] : 0;
         const bool act = pre_ok && s_live[mdl];
+        // first touch stores only on a full-force step; by increments
+        // every touch adds to the stored force
+        const uint32_t first_bit = s_direct[mdl] ? kFirstTouch : 0u;
         uint32_t cw[NG];
         float u0[NG], u1[NG], u2[NG];
 #pragma unroll
@@ -1056,7 +1141,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         if (act) {
 #pragma unroll
             for (int i = 0; i < NG; ++i)
-                if (!(cw[i] & kFirstTouch)) {
+                if (!(cw[i] & first_bit)) {
                     const float4* pf = reinterpret_cast<const float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld;
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(pf));
                 }
@@ -1128,7 +1213,7 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         float4 of[NG];
 #pragma unroll
         for (int i = 0; i < NG; ++i)
-            of[i] = (act && !(cw[i] & kFirstTouch))
+            of[i] = (act && !(cw[i] & first_bit))
                         ? *(reinterpret_cast<const float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld)
                         : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();  // fluxes of the whole group
@@ -1177,10 +1262,11 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
 }
 
 // Predictor only (start of a run or after a state overwrite).
+// Nodes g >= hv_begin hold the half-step velocity (v + dt/2 a) in v.
 template <typename Real>
 __global__ void predict_kernel(long long n_node, int F, const double* u, const double* v, const Real* a,
                                Real* ut, double dt, double half_dt2, const uint8_t* node_model,
-                               const ModelConst* mc) {
+                               const ModelConst* mc, long long hv_begin) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long total = n_node * F;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
@@ -1192,7 +1278,8 @@ __global__ void predict_kernel(long long n_node, int F, const double* u, const d
             h = K.dt;
             h2 = K.half_dt2;
         }
-        ut[padded_index(g, f, F)] = (Real)(u[idx] + h * v[idx] + h2 * (double)a[idx]);
+        ut[padded_index(g, f, F)] =
+            g >= hv_begin ? (Real)(u[idx] + h * v[idx]) : (Real)(u[idx] + h * v[idx] + h2 * (double)a[idx]);
         if (f % 3 == 2) ut[padded_index(g, f, F) + 1] = Real(0);
     }
 }
@@ -1209,6 +1296,14 @@ struct RecArgs {
     const Real* a;
     long long n_node;
     Out* out;               // [NFLD][n_rec][NN][15]
+    // nodes g >= hv_begin hold the half-step velocity: a = f/m from the
+    // step's assembled force, v = w - dt/2 a
+    long long hv_begin;
+    const Real* force;      // [node][NFLD][4]
+    const Real* inv_mass;   // [node]
+    const uint8_t* node_model;
+    const ModelConst* mc;
+    double dt;
 };
 
 // Snapshot of the recording cells: strain from the gathered corrected
@@ -1258,14 +1353,52 @@ __global__ void record_kernel(RecArgs<Real, Out> A) {
         o[3] = (Out)(0.5 * (gr[0][1] + gr[1][0]));
         o[4] = (Out)(0.5 * (gr[0][2] + gr[2][0]));
         o[5] = (Out)(0.5 * (gr[1][2] + gr[2][1]));
-        for (int c = 0; c < 3; ++c) {
-            o[6 + c] = (Out)A.u[(size_t)g * F + d * 3 + c];
-            o[9 + c] = (Out)A.v[(size_t)g * F + d * 3 + c];
-            o[12 + c] = (Out)A.a[(size_t)g * F + d * 3 + c];
+        if ((long long)g >= A.hv_begin) {
+            const double h = A.node_model ? A.mc[A.node_model[g]].dt : A.dt;
+            const Real im = A.inv_mass[g];
+            for (int c = 0; c < 3; ++c) {
+                const double an = (double)(Real)(A.force[((size_t)g * NFLD + d) * 4 + c] * im);
+                o[6 + c] = (Out)A.u[(size_t)g * F + d * 3 + c];
+                o[9 + c] = (Out)(A.v[(size_t)g * F + d * 3 + c] - 0.5 * h * an);
+                o[12 + c] = (Out)an;
+            }
+        } else {
+            for (int c = 0; c < 3; ++c) {
+                o[6 + c] = (Out)A.u[(size_t)g * F + d * 3 + c];
+                o[9 + c] = (Out)A.v[(size_t)g * F + d * 3 + c];
+                o[12 + c] = (Out)A.a[(size_t)g * F + d * 3 + c];
+            }
         }
     }
 }
 
+
+// Half-step velocity state <-> (v, a) at the nodes g >= hv_begin.
+// to_full: v_out = w - dt/2 a, a_out = a with a = f/m from the assembled
+// force (a_from_force) or the stored a (state set since the last step);
+// otherwise (from_full): w = v + dt/2 a in place of v.  One thread per
+// (node, value).
+template <typename Real>
+__global__ void half_v_kernel(long long n_node, int F, long long hv_begin, bool to_full, bool a_from_force,
+                              double* v, const Real* a, const Real* force, const Real* inv_mass,
+                              const uint8_t* node_model, const ModelConst* mc, double dt, double* v_out,
+                              Real* a_out) {
+    const long long total = (n_node - hv_begin) * F;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long g = hv_begin + t / F;
+        const int f = (int)(t % F);
+        const size_t i = (size_t)g * F + f;
+        const double h = node_model ? mc[node_model[g]].dt : dt;
+        if (to_full) {
+            const double an = a_from_force ? (double)(Real)(force[padded_index(g, f, F)] * inv_mass[g]) : (double)a[i];
+            v_out[i] = v[i] - 0.5 * h * an;
+            a_out[i] = (Real)an;
+        } else {
+            v[i] = v[i] + 0.5 * h * (double)a[i];
+        }
+    }
+}
 
 // Recording nodes merged across the recording cells that share them (the
 // strain Green's-function extraction of postprocess/cpp/main.cpp:300-425):

@@ -913,6 +913,9 @@ gfb_status gfb_trainer_collect(gfb_trainer* t, gfb_solver* thin, gfb_solver* thi
     if (layer->n_net != t->n_net) return set_error(GFB_ERR_INVALID, "trainer: network count differs from the layer's");
     if (solver_layer(thin)) return set_error(GFB_ERR_STATE, "trainer: the thin solver must have no layer attached");
     LCU(cudaSetDevice(t->device));
+    // the replay reads and writes u, v, a at every node
+    gfb_status st0;
+    if ((st0 = solver_full_state(thin)) || (st0 = solver_full_state(thick))) return st0;
     DevMem mem;
     Boundary B;
     gfb_status st;

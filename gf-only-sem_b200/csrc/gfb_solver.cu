@@ -30,6 +30,15 @@ namespace {
 
 thread_local std::string g_err;
 
+// Steps between full evaluations of the element force on the FP32 path:
+// the steps between add the force of the predicted displacement's
+// increment.  Each full evaluation rounds the whole predicted displacement
+// to float, a perturbation the stiffness amplifies into the highest
+// (undamped) modes; by increments the rounded quantity is a step's change,
+// ~dt*omega smaller, and the periodic full evaluation keeps the float sum
+// of increments from drifting.
+constexpr int kRefreshSteps = 100;
+
 gfb_status fail(gfb_status st, const char* fmt, ...) {
     char buf[1024];
     va_list ap;
@@ -290,6 +299,18 @@ struct gfb_solver {
     int* d_live_cell_end = nullptr;     // [colour]
     long long* d_live_node_end = nullptr;  // [2]
     int *d_mlive = nullptr, *d_mstep = nullptr, *d_nsteps = nullptr, *d_nstf = nullptr;
+    // element force in full every `refresh` steps and by increments between
+    // (FP32 path; 1 = in full every step): per model this step's kind, the
+    // next step's kind and a one-shot request for a full step
+    int refresh = 1;
+    int *d_mdirect = nullptr, *d_mnext = nullptr, *d_force_direct = nullptr;
+    // plain nodes (device nodes >= hv_begin) keep the half-step velocity
+    // v + dt/2 a in v and no acceleration (FP32 path); a_in_force: the
+    // assembled force holds the last step's (a = f/m), else a is the stored
+    // one (state set since the last step)
+    bool half_v = false;
+    long long hv_begin = 0;
+    bool a_in_force = false;
     long long* d_stf_off = nullptr;
     void *d_mstf = nullptr, *d_stf_all = nullptr;
     bool use_graph = true;
@@ -496,6 +517,8 @@ void node_args(const gfb_solver* s, gfb::NodeArgs<Real>& A, gfb::NodePml<Real>& 
     A.mc = s->d_mc;
     A.mlive = s->d_mlive;
     A.live_node_end = s->d_live_node_end;  // null with one model
+    A.mnext = s->refresh > 1 ? s->d_mnext : nullptr;
+    A.half_v = s->half_v;
     P = gfb::NodePml<Real>{};
     if (s->node_pml) {
         P.coef = static_cast<const Real*>(s->npml_coef);
@@ -536,6 +559,7 @@ gfb_status launch_elem_t(gfb_solver* s, int c) {
     A.src_set = s->src_set;
     A.n_set = s->n_set;
     A.mlive = s->d_mlive;
+    A.mdirect = s->refresh > 1 ? s->d_mdirect : nullptr;
     A.mc = s->d_mc;
     for (int d = 0; d < gfb::kMaxFields; ++d) {
         A.dir[d] = s->dirs[d];
@@ -582,6 +606,7 @@ gfb_status launch_col_e(gfb_solver* s, int c) {
     A.src_set = s->src_set;
     A.n_set = s->n_set;
     A.mlive = s->d_mlive;
+    A.mdirect = s->refresh > 1 ? s->d_mdirect : nullptr;
     A.n_model = s->n_model;
     for (int d = 0; d < gfb::kMaxFields; ++d) {
         A.dir[d] = s->dirs[d];
@@ -684,6 +709,12 @@ gfb_status launch_record_o(gfb_solver* s, Out* out) {
     A.a = static_cast<const Real*>(s->a);
     A.n_node = s->n_node;
     A.out = out;
+    A.hv_begin = s->half_v ? s->hv_begin : s->n_node;
+    A.force = static_cast<const Real*>(s->force);
+    A.inv_mass = static_cast<const Real*>(s->inv_mass);
+    A.node_model = s->d_node_model;
+    A.mc = s->d_mc;
+    A.dt = s->dt;
     gfb::record_kernel<Real, NG, NFLD, Out><<<s->n_rec, S::NNP, 0, s->stream>>>(A);
     CU(cudaGetLastError());
     s->launches++;
@@ -847,14 +878,62 @@ gfb_status launch_predict_t(gfb_solver* s) {
     const double h = 0.5 * s->dt * s->dt * (1.0 - 2.0 * 0.0);
     gfb::predict_kernel<Real><<<grid_for(n, 256), 256, 0, s->stream>>>(
         (long long)s->n_node, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h,
-        s->d_node_model, s->d_mc);
+        s->d_node_model, s->d_mc, s->half_v ? s->hv_begin : (long long)s->n_node);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
 }
 
+// Half-step velocity state of the plain nodes to (v, a): into v_out / a_out,
+// or in place (v_out == v, a_out == a) when leaving the form for good.
+gfb_status half_v_to_full(gfb_solver* s, double* v_out, float* a_out) {
+    const long long total = (long long)(s->n_node - s->hv_begin) * s->F;
+    if (total <= 0) return GFB_OK;
+    gfb::half_v_kernel<float><<<grid_for(total, 256), 256, 0, s->stream>>>(
+        (long long)s->n_node, s->F, s->hv_begin, true, s->a_in_force, s->v, static_cast<const float*>(s->a),
+        static_cast<const float*>(s->force), static_cast<const float*>(s->inv_mass), s->d_node_model, s->d_mc, s->dt,
+        v_out, a_out);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+// (v, a) of the plain nodes to the half-step velocity, in place.
+gfb_status half_v_from_full(gfb_solver* s) {
+    const long long total = (long long)(s->n_node - s->hv_begin) * s->F;
+    if (total <= 0) return GFB_OK;
+    gfb::half_v_kernel<float><<<grid_for(total, 256), 256, 0, s->stream>>>(
+        (long long)s->n_node, s->F, s->hv_begin, false, false, s->v, static_cast<const float*>(s->a), nullptr,
+        nullptr, s->d_node_model, s->d_mc, s->dt, nullptr, nullptr);
+    CU(cudaGetLastError());
+    s->launches++;
+    return GFB_OK;
+}
+
+// Leave the half-step velocity form (the learned layer and its trainer read
+// and write v and a at any node): v and a in place, from here on.
+gfb_status leave_half_v(gfb_solver* s) {
+    if (!s->half_v) return GFB_OK;
+    gfb_status st = half_v_to_full(s, s->v, static_cast<float*>(s->a));
+    if (st) return st;
+    CU(cudaStreamSynchronize(s->stream));
+    s->half_v = false;
+    s->hv_begin = s->n_node;
+    if (s->gexec) {
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
+    return GFB_OK;
+}
+
+// The predicted displacement rewritten in full from u, v, a (the start of a
+// run, or after a state overwrite): the next step evaluates the element
+// force in full.
 gfb_status launch_predict(gfb_solver* s) {
-    return s->prec == GFB_FP64 ? launch_predict_t<double>(s) : launch_predict_t<float>(s);
+    gfb_status st = s->prec == GFB_FP64 ? launch_predict_t<double>(s) : launch_predict_t<float>(s);
+    if (st) return st;
+    if (s->refresh > 1) CU(cudaMemsetAsync(s->d_force_direct, 1, (size_t)s->n_model * sizeof(int), s->stream));
+    return GFB_OK;
 }
 
 // A snapshot: the recording cells' records [field][rec][NN][15], then the
@@ -1356,6 +1435,9 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         if ((st = put_int(&s->d_nstf, nstf))) return st;
         if ((st = put_int(&s->d_mstep, zero))) return st;
         if ((st = put_int(&s->d_mlive, one))) return st;
+        if ((st = put_int(&s->d_mdirect, one))) return st;
+        if ((st = put_int(&s->d_mnext, one))) return st;
+        if ((st = put_int(&s->d_force_direct, zero))) return st;
         if ((st = s->alloc(&s->d_stf_off, off.size()))) return st;
         if ((st = h2d(s, s->d_stf_off, off.data(), off.size() * 8))) return st;
         if ((st = upload(s, &s->d_stf_all, stf_all))) return st;
@@ -1465,7 +1547,8 @@ gfb_status launch_step_begin_t(gfb_solver* s) {
     const int blocks = (s->n_model + threads - 1) / threads;
     gfb::step_begin_kernel<Real><<<blocks, threads, 0, s->stream>>>(
         s->n_model, s->n_set, s->d_mstep, s->d_nsteps, s->d_nstf, s->d_stf_off, static_cast<const Real*>(s->d_stf_all),
-        static_cast<Real*>(s->d_mstf), s->d_mlive);
+        static_cast<Real*>(s->d_mstf), s->d_mlive, s->refresh, s->d_force_direct,
+        s->refresh > 1 ? s->d_mdirect : nullptr, s->d_mnext);
     CU(cudaGetLastError());
     s->launches++;
     if (s->d_live_cell_end) {
@@ -1594,6 +1677,7 @@ gfb_status one_step(gfb_solver* s, cudaEvent_t* ev) {
     }
     if (ev) CU(cudaEventRecord(ev[3], s->stream));
     s->step++;
+    s->a_in_force = true;
     return GFB_OK;
 }
 
@@ -1858,6 +1942,21 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     if (st) return st;
     CU(cudaStreamSynchronize(s->stream));
     clk.mark("device set-up");
+    // FP32 path: the element force of most steps from the predicted
+    // displacement's increment (see step_begin_kernel), where the C-PML
+    // term is added at the nodes (node form or none) and no node is
+    // finalised inside the element kernel
+    s->refresh = (s->prec == GFB_FP32 && (!s->has_cpml || s->node_pml) && !s->fuse &&
+                  !(c->flags & GFB_FLAG_DIRECT_FORCE))
+                     ? kRefreshSteps
+                     : 1;
+    // plain nodes in the half-step velocity form where nothing reads their
+    // (v, a) inside the step: the FP32 path with node-form or no C-PML, no
+    // legacy damping (it acts on v_n, solver.cpp:564-574), no node update in
+    // the element kernel
+    s->half_v = s->prec == GFB_FP32 && (!s->has_cpml || s->node_pml) && !s->fuse && !s->has_damping &&
+                !(c->flags & GFB_FLAG_DIRECT_FORCE);
+    s->hv_begin = s->half_v ? (s->node_pml ? s->n_pml_node : 0) : s->n_node;
     if ((c->flags & GFB_FLAG_AUTOTUNE) && (st = autotune(s.get()))) return st;
     CU(cudaDeviceSynchronize());
     clk.mark("autotune");
@@ -2057,6 +2156,8 @@ gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
     info->elem_blocks = use_col_kernel(s) ? s->col_blocks : s->pipe_blocks;
     info->elem_kernel = use_col_kernel(s) ? 1 : 0;
     info->cells_per_group = use_col_kernel(s) ? s->col_epb : 0;
+    info->force_refresh = s->refresh;
+    info->half_v = s->half_v ? 1 : 0;
     return GFB_OK;
 }
 
@@ -2091,16 +2192,33 @@ gfb_status gfb_get_state(gfb_solver* s, int32_t field, double* u, double* v, dou
         if ((st = d2h(s, tmp.data(), s->u, nF * 8))) return st;
         pick(u);
     }
+    // half-step velocity form: (v, a) of the plain nodes recovered into
+    // temporary device arrays (the C-PML nodes copied as they are)
+    double* dv = s->v;
+    void* da = s->a;
+    std::unique_ptr<DevBuf> tv, ta;
+    if (s->half_v && (v || a)) {
+        tv = std::make_unique<DevBuf>();
+        ta = std::make_unique<DevBuf>();
+        CU(cudaMalloc(&tv->p, nF * 8));
+        CU(cudaMalloc(&ta->p, nF * 4));
+        CU(cudaMemcpyAsync(tv->p, s->v, nF * 8, cudaMemcpyDeviceToDevice, s->stream));
+        CU(cudaMemcpyAsync(ta->p, s->a, nF * 4, cudaMemcpyDeviceToDevice, s->stream));
+        if ((st = half_v_to_full(s, static_cast<double*>(tv->p), static_cast<float*>(ta->p)))) return st;
+        CU(cudaStreamSynchronize(s->stream));
+        dv = static_cast<double*>(tv->p);
+        da = ta->p;
+    }
     if (v) {
-        if ((st = d2h(s, tmp.data(), s->v, nF * 8))) return st;
+        if ((st = d2h(s, tmp.data(), dv, nF * 8))) return st;
         pick(v);
     }
     if (a) {
         if (s->prec == GFB_FP64) {
-            if ((st = d2h(s, tmp.data(), s->a, nF * 8))) return st;
+            if ((st = d2h(s, tmp.data(), da, nF * 8))) return st;
         } else {
             std::vector<float> f(nF);
-            if ((st = d2h(s, f.data(), s->a, nF * 4))) return st;
+            if ((st = d2h(s, f.data(), da, nF * 4))) return st;
             for (size_t i = 0; i < nF; ++i) tmp[i] = f[i];
         }
         pick(a);
@@ -2117,6 +2235,7 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
     CU(cudaStreamSynchronize(s->stream));
     const size_t nF = (size_t)s->n_node * s->F;
     std::vector<double> tmp(nF);
+    gfb_status st0;
     auto put = [&](const double* src, void* dev, bool is_real_float) -> gfb_status {
         gfb_status st;
         if (is_real_float) {
@@ -2138,9 +2257,18 @@ gfb_status gfb_set_state(gfb_solver* s, int32_t field, int32_t step, const doubl
         return GFB_OK;
     };
     gfb_status st;
+    // half-step velocity form: the other fields' (v, a) first, so that the
+    // wavefield written here and the others are all (v, a) when converted
+    if (s->half_v) {
+        if ((st0 = half_v_to_full(s, s->v, static_cast<float*>(s->a)))) return st0;  // in place
+        CU(cudaStreamSynchronize(s->stream));
+        s->a_in_force = false;  // a now holds every field's acceleration
+    }
     if ((st = put(u, s->u, false))) return st;
     if ((st = put(v, s->v, false))) return st;
     if ((st = put(a, s->a, s->prec == GFB_FP32))) return st;
+    if (s->half_v && (st = half_v_from_full(s))) return st;
+    s->a_in_force = false;
     if (s->has_cpml && !s->node_pml) {
         const size_t es = s->prec == GFB_FP64 ? 8 : 4;
         CU(cudaMemset(s->pml_mem, 0, (size_t)s->n_pml * s->F * 3 * s->nn * es));
@@ -2180,6 +2308,11 @@ std::vector<std::pair<void*, size_t>> checkpoint_arrays(gfb_solver* s) {
         a.push_back({s->npml_prev, (size_t)s->n_pml_node * s->F * es});
     }
     a.push_back({s->d_mstep, (size_t)s->n_model * 4});
+    if (s->refresh > 1) {
+        // the stored force is state when it is updated by increments
+        a.push_back({s->force, (size_t)s->n_node * s->nfld * 4 * es});
+        a.push_back({s->d_force_direct, (size_t)s->n_model * 4});
+    }
     return a;
 }
 
@@ -2189,6 +2322,7 @@ struct CheckpointHeader {
     int32_t version, precision, n_field, n_model;
     int64_t n_node, n_cell, n_pml, n_pml_node;
     int32_t step, flags;
+    int32_t half_v, a_in_force;
 };
 
 void checkpoint_header(const gfb_solver* s, int64_t bytes, CheckpointHeader& h) {
@@ -2205,6 +2339,8 @@ void checkpoint_header(const gfb_solver* s, int64_t bytes, CheckpointHeader& h) 
     h.n_pml_node = s->node_pml ? s->n_pml_node : 0;
     h.step = s->step;
     h.flags = s->flags;
+    h.half_v = s->half_v ? 1 : 0;
+    h.a_in_force = s->a_in_force ? 1 : 0;
 }
 
 }  // namespace
@@ -2245,6 +2381,7 @@ gfb_status gfb_checkpoint_load(gfb_solver* s, const void* buf, int64_t bytes) {
     std::memcpy(&h, buf, sizeof(h));
     checkpoint_header(s, need, mine);
     mine.step = h.step;
+    mine.a_in_force = h.a_in_force;
     if (std::memcmp(&h, &mine, sizeof(h)) != 0 || bytes < need)
         return fail(GFB_ERR_INVALID, "checkpoint does not belong to a solver built like this one");
     CU(cudaSetDevice(s->device));
@@ -2255,6 +2392,7 @@ gfb_status gfb_checkpoint_load(gfb_solver* s, const void* buf, int64_t bytes) {
         p += a.second;
     }
     s->step = h.step;
+    s->a_in_force = h.a_in_force != 0;
     return GFB_OK;
 }
 
@@ -2485,11 +2623,24 @@ SolverView solver_view(gfb_solver* s) {
 
 gfb_status solver_predict(gfb_solver* s) { return launch_predict(s); }
 
+gfb_status solver_full_state(gfb_solver* s) { return leave_half_v(s); }
+
 Layer* solver_layer(gfb_solver* s) { return s->layer; }
 
 gfb_status solver_set_layer(gfb_solver* s, Layer* layer) {
     if (s->layer) layer_free(s->layer);
     s->layer = layer;
+    if (layer) {
+        gfb_status st = leave_half_v(s);
+        if (st) return st;
+    }
+    if (layer && s->refresh > 1) {
+        // the layer adds its correction to the assembled force each step,
+        // which must not accumulate: the force is evaluated in full from now
+        s->refresh = 1;
+        gfb_status st = launch_predict(s);
+        if (st) return st;
+    }
     // the captured step graph does not contain the layer's launch
     if (s->gexec) {
         cudaGraphExecDestroy(s->gexec);

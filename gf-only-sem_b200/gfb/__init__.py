@@ -29,6 +29,7 @@ FLAG_FUSED_NODE = 4
 FLAG_POINT_KERNEL = 8
 FLAG_NO_GRAPH = 16
 FLAG_AUTOTUNE = 32
+FLAG_DIRECT_FORCE = 64
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -93,6 +94,8 @@ class Info(C.Structure):
         ("elem_blocks", C.c_int32),
         ("elem_kernel", C.c_int32),
         ("cells_per_group", C.c_int32),
+        ("force_refresh", C.c_int32),
+        ("half_v", C.c_int32),
     ]
 
 

@@ -111,6 +111,17 @@ typedef struct gfb_config {
  * the fastest; gfb_get_info reports the choice.  Tuning leaves the state
  * unchanged. */
 #define GFB_FLAG_AUTOTUNE 32
+/* FP32 path: evaluate the element force from the full predicted
+ * displacement at every step.  By default most steps add the force of the
+ * predicted displacement's increment over the previous step to the stored
+ * force, with a full evaluation every 100 steps (and after the state is
+ * overwritten): the float rounding of the full predicted displacement,
+ * amplified by the stiffness into the highest modes, is what bounds the
+ * FP32 path's accuracy (recorded acceleration ~1.5e-4 relative L2 after
+ * 2000 steps in full, ~3e-5 by increments).  Applies only where the C-PML
+ * term is added at the nodes or there is none, and without a learned layer
+ * or GFB_FLAG_FUSED_NODE (those evaluate in full every step). */
+#define GFB_FLAG_DIRECT_FORCE 64
 
 /* Point-force source (config.h5 /source, io.cpp:681-707). */
 typedef struct gfb_source {
@@ -244,6 +255,8 @@ typedef struct gfb_info {
     int32_t elem_blocks;     /* blocks in the persistent grid of the element kernel in use  */
     int32_t elem_kernel;     /* 1: thread-per-xi-line kernel, 0: thread-per-point kernel    */
     int32_t cells_per_group; /* cells per block iteration of the line kernel (0 otherwise)  */
+    int32_t force_refresh;   /* steps between full element-force evaluations (1: every step) */
+    int32_t half_v;          /* 1: plain nodes keep the half-step velocity, no acceleration */
 } gfb_info;
 
 gfb_status gfb_get_info(const gfb_solver* solver, gfb_info* info);

@@ -240,8 +240,9 @@ def test_fused_node_update_equals_separate_pass(prec):
     prob = layered_problem(nsteps=70)
     runs = []
     # the fused update lives in the thread-per-point kernel; compare with the
-    # same kernel and a separate node pass
-    for flags in (gfb.FLAG_POINT_KERNEL, gfb.FLAG_FUSED_NODE):
+    # same kernel and a separate node pass, both evaluating the element force
+    # in full every step (the fused update always does)
+    for flags in (gfb.FLAG_POINT_KERNEL | gfb.FLAG_DIRECT_FORCE, gfb.FLAG_FUSED_NODE):
         s = gfb.Solver(prob, dirs=[0, 1, 2], precision=prec, flags=flags)
         s.advance(70)
         runs.append((s.drain(), [s.state(f) for f in range(3)]))
@@ -400,3 +401,35 @@ def test_source_sets_are_checked():
         gfb.Solver(prob, dirs=[0, 1, 2, 0], precision=gfb.FP32, sources=sources, field_source=[0, 0, 0, 1])
     with pytest.raises(gfb.GfbError):
         gfb.Solver(prob, dirs=[0, 1], precision=gfb.FP32, sources=sources, field_source=[0, 2])
+
+
+def test_fp32_force_by_increments_against_full_evaluation():
+    """FP32 path: the element force of most steps is the stored force plus
+    the force of the predicted displacement's increment (full evaluation
+    every 100 steps, and after a state overwrite); evaluating it in full
+    every step (GFB_FLAG_DIRECT_FORCE) gives the same traces to FP32 rounding,
+    both within 1e-4 of the FP64 oracle, and a resume through set_state
+    continues correctly."""
+    prob = layered_problem(nsteps=260)
+    n = prob["nsteps"]
+    inc = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32)
+    full = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, flags=gfb.FLAG_DIRECT_FORCE)
+    inc.advance(n)
+    full.advance(n)
+    a, b = inc.drain(), full.drain()
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(a[d], ref, FP32_TOL, f"increments field {d}")
+        compare_runs(b[d], ref, FP32_TOL, f"full field {d}")
+    # state overwrite mid-run: the next step is a full evaluation
+    half = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, record=False)
+    half.advance(130)
+    st = [half.state(f) for f in range(3)]
+    res = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, record=False)
+    for f in range(3):
+        res.set_state(f, 130, *st[f])
+    res.advance(130)
+    inc2 = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, record=False)
+    inc2.advance(260)
+    for f in range(3):
+        assert rel_l2(res.state(f)[0], inc2.state(f)[0]) < FP32_TOL
