@@ -461,7 +461,7 @@ def node_bytes_per_step(prob, info, n_field, prec):
 
 
 def committed_traffic():
-    path = os.path.join(REPO, "profiles", "elem_step_traffic.json")
+    path = os.path.join(REPO, "profiles", "elem_col_traffic_deformed_32x32x16.json")
     try:
         with open(path) as f:
             return json.load(f)
