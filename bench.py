@@ -57,9 +57,11 @@ BATCH = dict(n_model=32, seed=4, d=250.0, pml=4, nmin=(16, 16, 8), nmax=(48, 48,
 LAYER = {
     "layer96": dict(ni=94, nk=47, d=250.0, seed=2, steps=2000, stride=50,
                     train_pairs=24, train_ni=10, train_nk=6, train_steps=700, epochs=30,
+                    loop_cases=3, loop_ni=16, loop_nk=8, loop_steps=800, loop_evals=100,
                     val_ni=22, val_nk=11, val_steps=900),
     "layer24": dict(ni=22, nk=11, d=250.0, seed=2, steps=900, stride=10,
                     train_pairs=6, train_ni=8, train_nk=5, train_steps=500, epochs=15,
+                    loop_cases=3, loop_ni=12, loop_nk=6, loop_steps=600, loop_evals=80,
                     val_ni=16, val_nk=8, val_steps=600),
 }
 
@@ -194,53 +196,42 @@ def run_layer(args):
     samples = int(tr.samples().sum())
     tr.close()
 
-    def run(prob, weights=None, scale_mult=1.0, n_steps=None):
-        """Step prob (with the layer when weights are given, its output scale
-        times scale_mult) and keep the recorded displacement (float32: the
-        compared quantity, and small enough for 96 x 96 surface cells)."""
-        import ctypes as C
-
-        n_steps = n_steps or int(prob["nsteps"])
-        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, device=args.device, record_slots=16,
-                       flags=gfb.FLAG_RECORD_F32)
-        if weights is not None:
-            sc = np.array(scales, dtype=np.float32)
-            sc[3] *= scale_mult
-            gl.attach(s, gl.Layer(prob), weights, sc, threshold=0.05)
-        us = {f: [] for f in range(3)}
-        step = C.c_int32()
-        null = C.cast(None, C.POINTER(C.c_double))
-
-        def read_all():
-            while s.pending() > 0:
-                for f in range(3):
-                    u = np.zeros((s.n_rec, s.nn, 3))
-                    gfb._check(s.lib.gfb_read_record(s.h, f, C.byref(step), null,
-                                                     u.ctypes.data_as(C.POINTER(C.c_double)), null, null, 0))
-                    us[f].append(u.astype(np.float32))
-
-        ms = 0.0
-        done = 0
-        while done < n_steps:
-            k = min(200, n_steps - done)
-            ms += s.advance_timed(k)
-            read_all()
-            done += k
-        st = gl.status(s) if weights is not None else None
-        s.close()
-        snaps = {f: {"u": np.stack(us[f])} for f in range(3)}
-        return snaps, ms / n_steps, st
+    def run(prob, weights=None, scale_mult=1.0, gains=None, planes=None):
+        """Step prob with the layer when weights are given (its output
+        scale times scale_mult, damping gains `gains`, nodes on the depth
+        `planes`) and keep the recorded displacement (float32)."""
+        return gl.run_domain(prob, weights, scales, gains, scale_mult, device=args.device, planes=planes)
 
     def rms(x):
         return float(np.sqrt(np.mean(np.square(x))))
 
-    # closed-loop selection on held-out models: the one-step replay loss the
-    # networks are fitted to is not the reflection error, so the candidates
-    # (trained or untrained weights, output scale x 0.25 .. 4) are compared
-    # by the reflection error they give when stepping two validation models
-    # (seeds of neither the training nor the test model), and the best is
-    # the layer that goes to the test model
     zero = params * 0.0  # untrained: constant damping softplus(0) on every axis
+    # closed-loop stage of training: damping gains per network and face axis
+    # fitted to the reflection error of whole runs of further training
+    # models (their thick-C-PML runs are the targets), for the untrained and
+    # for the replay-trained networks
+    t0 = time.perf_counter()
+    cases = [gl.loop_case(pair(3000 + k, w["loop_ni"], w["loop_nk"], w["loop_steps"]), device=args.device)
+             for k in range(w["loop_cases"])]
+    fits = {}
+    all_planes = tuple(range(5))
+    for name, wts, planes in (("untrained", zero, None), ("trained", params, None),
+                              ("untrained, 5 planes", zero, all_planes)):
+        g, e, hist = gl.fit_gains(cases, wts, scales, max_evals=w["loop_evals"] * (3 if planes else 1),
+                                  device=args.device, planes=planes)
+        fits[name] = dict(gains=g, train_error=e, start_error=hist[0][1], evals=hist[-1][0], planes=planes,
+                          weights=wts)
+    for c in cases:
+        c.close()
+    del cases
+    t_loop = time.perf_counter() - t0
+
+    # selection on held-out models: the candidates (replay-trained or
+    # untrained networks at output scale x 0.25 .. 4 with unit gains, and
+    # each network with its closed-loop gains) are compared by the
+    # reflection error they give when stepping two validation models (seeds
+    # of none of the training models nor the test model), and the best is
+    # the layer that goes to the test model
     t0 = time.perf_counter()
     val = []
     for vseed in (5000, 5001):
@@ -250,18 +241,19 @@ def run_layer(args):
         keys, dtv = gl.surface_keys(thv), thv["dt"]
         del thv
         val.append((pv, gl.build_domain(pv, pv.n_thin, dtv), keys, thv_rec))
-    cands = [(wname, wts, k) for wname, wts in (("trained", params), ("untrained", zero))
+    cands = [(wname, wts, k, None, None) for wname, wts in (("trained", params), ("untrained", zero))
              for k in (0.25, 0.5, 1.0, 2.0, 4.0)]
+    cands += [(f"{name} + closed-loop gains", f["weights"], 1.0, f["gains"], f["planes"]) for name, f in fits.items()]
     scores = []
-    for wname, wts, k in cands:
+    for wname, wts, k, g, planes in cands:
         errs = []
         for pv, tn, keys, thv_rec in val:
-            rec, _, _ = run(tn, wts, k)
+            rec, _, _ = run(tn, wts, k, g, planes)
             errs += [gl.reflection_error(tn, rec[f], keys, thv_rec[f], (pv.n_thick - pv.n_thin) * d)
                      for f in range(3)]
         scores.append(rms(errs))
     best = int(np.argmin(scores))
-    sel_name, sel_w, sel_k = cands[best]
+    sel_name, sel_w, sel_k, sel_g, sel_planes = cands[best]
     t_select = time.perf_counter() - t0
     del val
 
@@ -275,14 +267,16 @@ def run_layer(args):
     del thick
     thin = gl.build_domain(p, p.n_thin, dt)
     plain, ms_plain, _ = run(thin)
-    selected, ms_learned, st = run(thin, sel_w, sel_k)
+    selected, ms_learned, st = run(thin, sel_w, sel_k, sel_g, sel_planes)
     trained_k1, _, _ = run(thin, params, 1.0)
     untrained, _, _ = run(thin, zero, 1.0)
+    loops = {name: run(thin, f["weights"], 1.0, f["gains"], f["planes"])[0] for name, f in fits.items()}
 
     def errs_of(snaps):
         return [gl.reflection_error(thin, snaps[f], thick_keys, thick_rec[f], shift) for f in range(3)]
 
     err_plain, err_sel, err_trained, err_untrained = (errs_of(x) for x in (plain, selected, trained_k1, untrained))
+    err_loops = {name: errs_of(x) for name, x in loops.items()}
     value = rms(err_sel)
     line = {
         "metric": "reflection error of a learned 1-element absorbing layer vs a 10-element C-PML "
@@ -295,14 +289,22 @@ def run_layer(args):
                    "train_pairs": w["train_pairs"], "train_samples": samples, "epochs": w["epochs"],
                    "loss_zero_prediction": base, "loss_first_epoch": float(loss[0]) if len(loss) else None,
                    "loss_last_epoch": float(loss[-1]) if len(loss) else None,
-                   "collect_s": t_collect, "fit_s": t_fit, "select_s": t_select},
+                   "collect_s": t_collect, "fit_s": t_fit, "closed_loop_s": t_loop, "select_s": t_select},
+        "closed_loop": {"on": f"{w['loop_cases']} training models {w['loop_ni']}x{w['loop_ni']}x{w['loop_nk']} "
+                              f"cells, {w['loop_steps']} steps",
+                        **{name: {"gains": {f"net {k}": [float(x) for x in f["gains"][k]]
+                                            for k in sorted(set(int(q) for q in gl.Layer(thin, f["planes"]).net))},
+                                  "train_error_start": f["start_error"], "train_error_fitted": f["train_error"],
+                                  "evaluations": f["evals"]} for name, f in fits.items()}},
         "selection": {"on": f"2 held-out models {w['val_ni']}x{w['val_ni']}x{w['val_nk']} cells, "
                             f"{w['val_steps']} steps",
-                      "chosen": {"weights": sel_name, "output_scale_x": sel_k},
+                      "chosen": {"weights": sel_name, "output_scale_x": sel_k,
+                                 "depth_planes": list(sel_planes) if sel_planes else [4]},
                       "validation_error": {f"{c[0]} x{c[2]}": sc for c, sc in zip(cands, scores)}},
         "reflection_error": {"learned_selected": err_sel, "thin_cpml_only": err_plain,
                              "trained_network_scale_x1": err_trained,
-                             "untrained_network_constant_damping": err_untrained},
+                             "untrained_network_constant_damping": err_untrained,
+                             **{f"{name} + closed-loop gains": e for name, e in err_loops.items()}},
         "ms_per_step": {"thick_cpml": ms_thick, "thin_cpml_only": ms_plain, "thin_learned": ms_learned},
         "layer_active_at_end": bool(st[0]) if st else None, "monitored_residual": st[1] if st else None,
     }

@@ -643,6 +643,48 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Bulk copies (TMA, no tensor map, no multicast) completing on an mbarrier
+// of this block: one thread announces the bytes of a stage and issues its
+// copies; every thread waits for the phase with a bounded poll.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// The phase of parity `parity` completed; false after kMbarPolls polls
+// (each try_wait may suspend the thread for a while), which only a lost
+// copy would cause.
+constexpr long kMbarPolls = 1L << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (long k = 0; k < kMbarPolls; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+// bytes: a multiple of 16; both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_copy_g2s(void* smem, const void* gmem, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_u32(smem)), "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 template <typename Real, int NG, int NFLD>
 struct PipeShape {
     static constexpr int NN = NG * NG * NG;
@@ -1001,10 +1043,14 @@ struct ColArgs {
     int n_model;                   // <= kMaxModels
     int dir[kMaxFields];
     int fset[kMaxFields];
+    unsigned* err;                 // set to 1 when a bulk copy's wait gave up (the launch did not finish)
     float D[36];                   // D[i*NG+s], read with compile-time indices only
 };
 
-template <int NG, int NFLD, int EPB_>
+// TMA: the geometry and node-table stages are filled by bulk copies (one per
+// cell, issued by one thread, completing on a per-stage mbarrier) instead of
+// 16-byte cp.async by every thread.
+template <int NG, int NFLD, int EPB_, bool TMA = false>
 __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<NG, NFLD, EPB_>::THREADS <= 160 ? 3 : 2))
     elem_col_kernel(ColArgs A) {
     using S = ColShape<NG, NFLD, EPB_>;
@@ -1089,19 +1135,70 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                       : make_float4(0.f, 0.f, 0.f, 0.f);
     };
 
+    // bulk-copy stages: barriers 0, 1 for the geometry, 2..4 for the node table
+    __shared__ __align__(8) uint64_t s_bar[5];
+    auto tma_geo = [&](int grp, int st) {
+        if (tid != 0) return;
+        const int e0 = A.e_begin + grp * EPB, nc = min(EPB, e_end - e0);
+        fence_proxy_async_smem();
+        mbar_expect_tx(&s_bar[st], (unsigned)(nc * S::GEO_B));
+        for (int c = 0; c < nc; ++c)
+            bulk_copy_g2s(gbase + (st * EPB + c) * S::GEO_SLOT,
+                          reinterpret_cast<const unsigned char*>(A.geom) + (size_t)(e0 + c) * S::GEO_B, S::GEO_B,
+                          &s_bar[st]);
+    };
+    auto tma_ib = [&](int grp, int st) {
+        if (tid != 0) return;
+        const int e0 = A.e_begin + grp * EPB, nc = min(EPB, e_end - e0);
+        fence_proxy_async_smem();
+        mbar_expect_tx(&s_bar[2 + st], (unsigned)(nc * S::IB_B));
+        for (int c = 0; c < nc; ++c)
+            bulk_copy_g2s(ibase + (st * EPB + c) * S::IB_B,
+                          reinterpret_cast<const unsigned char*>(A.ibool_padded) + (size_t)(e0 + c) * S::IB_B,
+                          S::IB_B, &s_bar[2 + st]);
+    };
+    // a wait that gave up: flag it, give the copies in flight a second
+    // bounded wait, and leave (every thread together)
+    auto give_up = [&](int b0, unsigned p0, int b1, unsigned p1) {
+        if (tid == 0) {
+            atomicOr(A.err, 1u);
+            if (b0 >= 0) mbar_wait(&s_bar[b0], p0);
+            if (b1 >= 0) mbar_wait(&s_bar[b1], p1);
+        }
+    };
+
     const int G = gridDim.x;
     const int grp0 = blockIdx.x;
-    if (grp0 < n_groups) issue_ib(grp0, 0);
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
+    if constexpr (TMA) {
+        if (tid == 0) {
+            for (int b = 0; b < 5; ++b) mbar_init(&s_bar[b], 1);
+            mbar_init_fence();
+        }
+        __syncthreads();
+        if (grp0 < n_groups) tma_ib(grp0, 0);
+        const bool bad = grp0 < n_groups && !mbar_wait(&s_bar[2], 0);
+        if (__syncthreads_or(bad)) {
+            give_up(2, 0, -1, 0);
+            return;
+        }
+    } else {
+        if (grp0 < n_groups) issue_ib(grp0, 0);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+    }
     uint32_t nw[NG];
     float4 pre[NG];
     bool pre_ok = line_nodes(grp0, 0, nw);
     load_vectors(nw, pre_ok, pre);
-    if (grp0 < n_groups) issue_geo(grp0, 0);
-    if (grp0 + G < n_groups) issue_ib(grp0 + G, 1);
-    cp_async_commit();
+    if constexpr (TMA) {
+        if (grp0 < n_groups) tma_geo(grp0, 0);
+        if (grp0 + G < n_groups) tma_ib(grp0 + G, 1);
+    } else {
+        if (grp0 < n_groups) issue_geo(grp0, 0);
+        if (grp0 + G < n_groups) issue_ib(grp0 + G, 1);
+        cp_async_commit();
+    }
 
     const int ubase = line * SP + col;        // + c*GR*SP + i*NG2
     const int ebase = line * SP + col - j * NG;  // + s*NG  (eta line: i*NG2 + s*NG + k)
@@ -1129,12 +1226,27 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                 us[2 * GR * SP + ubase + i * NG2] = u2[i];
             }
         }
-        cp_async_wait_all();
-        __syncthreads();  // displacement of this group, its geometry, the next node table
         const int nx = grp + G;
-        if (nx < n_groups) issue_geo(nx, (it + 1) & 1);
-        if (nx + G < n_groups) issue_ib(nx + G, (it + 2) % 3);
-        cp_async_commit();
+        if constexpr (TMA) {
+            // stage it&1 holds this group's geometry (use it/2 of that stage),
+            // stage (it+1)%3 the next group's node table (use (it+1)/3)
+            const unsigned pg = (unsigned)(it >> 1) & 1u, pi = (unsigned)((it + 1) / 3) & 1u;
+            const int bi = nx < n_groups ? 2 + (it + 1) % 3 : -1;
+            bool bad = !mbar_wait(&s_bar[it & 1], pg);
+            if (bi >= 0) bad = !mbar_wait(&s_bar[bi], pi) || bad;
+            if (__syncthreads_or(bad)) {  // displacement of this group, its geometry, the next node table
+                give_up(it & 1, pg, bi, pi);
+                return;
+            }
+            if (nx < n_groups) tma_geo(nx, (it + 1) & 1);
+            if (nx + G < n_groups) tma_ib(nx + G, (it + 2) % 3);
+        } else {
+            cp_async_wait_all();
+            __syncthreads();  // displacement of this group, its geometry, the next node table
+            if (nx < n_groups) issue_geo(nx, (it + 1) & 1);
+            if (nx + G < n_groups) issue_ib(nx + G, (it + 2) % 3);
+            cp_async_commit();
+        }
         // old force vectors of the nodes this colour does not touch first:
         // start their DRAM reads into L2 now, so the loads issued after the
         // flux phase find them there (no registers held meanwhile)

@@ -145,6 +145,7 @@ struct LayerArgs {
     int n_net;
     const __nv_bfloat16* w;   // [n_net][kWNet]
     float sc[4];              // channel scales u, v, a; output scale
+    const float* gain;        // [n_net][3] damping gain per network and face axis
     const double* u;
     const double* v;
     const float* a;
@@ -338,7 +339,8 @@ __global__ void __launch_bounds__(kLayerWarps * 32) layer_kernel(LayerArgs A) {
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
                     const int ax = frame_axis(oframe, j);
-                    float dj = gain * sl[j];  // non-finite stays non-finite (the monitor's signal)
+                    // non-finite stays non-finite (the monitor's signal)
+                    float dj = gain * __ldg(A.gain + net * 3 + j) * sl[j];
                     if (isfinite(dj)) dj = fminf(dj, cap);
                     // trapezoidal dashpot: velocity at the end of the step
                     // estimated from this step's force, the damping taken
@@ -464,6 +466,8 @@ struct Layer {
     Boundary B;
     __nv_bfloat16* w = nullptr;
     float sc[4] = {1.f, 1.f, 1.f, 1.f};
+    float* gain = nullptr;      // [n_net][3]
+    int n_net = 0;
     double* acc = nullptr;      // [4]
     double* monitor = nullptr;  // [3]
     int* active = nullptr;
@@ -483,6 +487,7 @@ gfb_status launch_layer(const SolverView& v, Layer* L) {
     A.n_net = L->B.n_net;
     A.w = L->w;
     for (int q = 0; q < 4; ++q) A.sc[q] = L->sc[q];
+    A.gain = L->gain;
     A.u = v.u;
     A.v = v.v;
     A.a = static_cast<const float*>(v.a);
@@ -807,6 +812,12 @@ gfb_status gfb_layer_attach(gfb_solver* s, const gfb_layer* layer, const uint16_
         if (!(scales[q] > 0.f)) return set_error(GFB_ERR_INVALID, "learned layer: scales must be positive");
         L->sc[q] = scales[q];
     }
+    L->n_net = layer->n_net;
+    if ((st = L->mem.alloc(&L->gain, (size_t)layer->n_net * 3))) return st;
+    {
+        const std::vector<float> ones((size_t)layer->n_net * 3, 1.f);
+        LCU(cudaMemcpy(L->gain, ones.data(), ones.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     if ((st = L->mem.alloc(&L->acc, 4))) return st;
     if ((st = L->mem.alloc(&L->monitor, 3))) return st;
     if ((st = L->mem.alloc(&L->active, 1))) return st;
@@ -831,6 +842,22 @@ gfb_status gfb_layer_attach(gfb_solver* s, const gfb_layer* layer, const uint16_
     if (per_sm < 1) return set_error(GFB_ERR_UNSUPPORTED, "learned layer: kernel does not fit on an SM");
     L->blocks = std::max(1, std::min(per_sm * n_sm, (L->B.n_tile + kLayerWarps - 1) / kLayerWarps));
     return solver_set_layer(s, L.release());
+}
+
+gfb_status gfb_layer_set_gains(gfb_solver* s, int32_t n_net, const float* gains) {
+    using namespace gfb;
+    if (!s || !gains) return set_error(GFB_ERR_INVALID, "NULL argument");
+    Layer* L = solver_layer(s);
+    if (!L) return set_error(GFB_ERR_STATE, "no learned layer attached");
+    if (n_net != L->n_net) return set_error(GFB_ERR_INVALID, "learned layer: gains for another network count");
+    for (int q = 0; q < 3 * n_net; ++q)
+        if (!(gains[q] >= 0.f) || !std::isfinite(gains[q]))
+            return set_error(GFB_ERR_INVALID, "learned layer: gains must be finite and >= 0");
+    const SolverView v = solver_view(s);
+    LCU(cudaSetDevice(v.device));
+    LCU(cudaStreamSynchronize(v.stream));
+    LCU(cudaMemcpy(L->gain, gains, (size_t)n_net * 3 * sizeof(float), cudaMemcpyHostToDevice));
+    return GFB_OK;
 }
 
 gfb_status gfb_layer_status(gfb_solver* s, int32_t* active, double* residual) {

@@ -304,6 +304,7 @@ struct gfb_solver {
     // next step's kind and a one-shot request for a full step
     int refresh = 1;
     int *d_mdirect = nullptr, *d_mnext = nullptr, *d_force_direct = nullptr;
+    int* d_kernel_err = nullptr;       // set by a kernel whose bounded wait gave up
     // plain nodes (device nodes >= hv_begin) keep the half-step velocity
     // v + dt/2 a in v and no acceleration (FP32 path); a_in_force: the
     // assembled force holds the last step's (a = f/m), else a is the stored
@@ -583,7 +584,7 @@ bool col_kernel_eligible(const gfb_solver* s) {
 }
 bool use_col_kernel(const gfb_solver* s) { return col_kernel_eligible(s) && !s->point_kernel; }
 
-template <int NG, int NFLD, int EPB>
+template <int NG, int NFLD, int EPB, bool TMA = false>
 gfb_status launch_col_e(gfb_solver* s, int c) {
     using S = gfb::ColShape<NG, NFLD, EPB>;
     gfb::ColArgs A;
@@ -614,7 +615,8 @@ gfb_status launch_col_e(gfb_solver* s, int c) {
     }
     for (int q = 0; q < 36; ++q) A.D[q] = q < NG * NG ? s->dmat_host[q] : 0.f;
     const int blocks = std::max(1, std::min(A.n_groups, s->col_blocks));
-    gfb::elem_col_kernel<NG, NFLD, EPB><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
+    A.err = reinterpret_cast<unsigned*>(s->d_kernel_err);
+    gfb::elem_col_kernel<NG, NFLD, EPB, TMA><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -629,7 +631,7 @@ struct ColEpb {
     static constexpr int D = gfb::col_default_epb(NG, NFLD);
     // the fewer / more cells-per-group variants exist for ngll 5 with up to
     // three wavefields (more would exceed a block's threads)
-    static constexpr int N = (NG == 5 && NFLD <= 3) ? 3 : 1;
+    static constexpr int N = (NG == 5 && NFLD <= 3) ? 4 : 1;
 };
 
 template <int NG, int NFLD>
@@ -638,17 +640,19 @@ gfb_status launch_col_t(gfb_solver* s, int c) {
     if constexpr (E::N > 1) {
         if (s->col_variant == 1) return launch_col_e<NG, NFLD, col_epb_lo(NFLD)>(s, c);
         if (s->col_variant == 2) return launch_col_e<NG, NFLD, col_epb_hi(NFLD)>(s, c);
+        if (s->col_variant == 3) return launch_col_e<NG, NFLD, E::D, true>(s, c);
     }
     return launch_col_e<NG, NFLD, E::D>(s, c);
 }
 
 // Persistent grid of the line kernel variant EPB: occupancy x SMs.
-template <int NG, int NFLD, int EPB>
+template <int NG, int NFLD, int EPB, bool TMA = false>
 gfb_status col_grid(gfb_solver* s, int* blocks) {
     using C = gfb::ColShape<NG, NFLD, EPB>;
-    CU(cudaFuncSetAttribute(gfb::elem_col_kernel<NG, NFLD, EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    auto* fn = gfb::elem_col_kernel<NG, NFLD, EPB, TMA>;
+    CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
     int per_sm = 0, n_sm = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gfb::elem_col_kernel<NG, NFLD, EPB>, C::THREADS, C::SMEM));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, C::THREADS, C::SMEM));
     CU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->device));
     if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "line element kernel does not fit on an SM");
     *blocks = per_sm * n_sm;
@@ -668,6 +672,10 @@ gfb_status col_grid_t(gfb_solver* s) {
         if (s->col_variant == 2) {
             s->col_epb = col_epb_hi(NFLD);
             return col_grid<NG, NFLD, col_epb_hi(NFLD)>(s, &s->col_blocks);
+        }
+        if (s->col_variant == 3) {
+            s->col_epb = E::D;
+            return col_grid<NG, NFLD, E::D, true>(s, &s->col_blocks);
         }
     }
     if ((st = col_grid<NG, NFLD, E::D>(s, &s->col_blocks))) return st;
@@ -1438,6 +1446,7 @@ gfb_status build_device(gfb_solver* s, const gfb_mesh* m, const gfb_source* src,
         if ((st = put_int(&s->d_mdirect, one))) return st;
         if ((st = put_int(&s->d_mnext, one))) return st;
         if ((st = put_int(&s->d_force_direct, zero))) return st;
+        if ((st = put_int(&s->d_kernel_err, std::vector<int>(1, 0)))) return st;
         if ((st = s->alloc(&s->d_stf_off, off.size()))) return st;
         if ((st = h2d(s, s->d_stf_off, off.data(), off.size() * 8))) return st;
         if ((st = upload(s, &s->d_stf_all, stf_all))) return st;
@@ -2068,6 +2077,18 @@ gfb_status gfb_destroy(gfb_solver* s) {
     return GFB_OK;
 }
 
+namespace {
+// A kernel whose bounded wait on its own bulk copies gave up left the step
+// unfinished: report it at the next synchronisation.
+gfb_status check_kernel_err(gfb_solver* s) {
+    if (!s->d_kernel_err) return GFB_OK;
+    int e = 0;
+    CU(cudaMemcpy(&e, s->d_kernel_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(GFB_ERR_CUDA, "element kernel: a bulk copy did not complete; the state is invalid");
+    return GFB_OK;
+}
+}  // namespace
+
 gfb_status gfb_advance(gfb_solver* s, int32_t n_steps) {
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (n_steps < 0) return fail(GFB_ERR_INVALID, "n_steps must be >= 0");
@@ -2099,7 +2120,7 @@ gfb_status gfb_advance_timed(gfb_solver* s, int32_t n_steps, double* ms) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (!st && ms) *ms += t;
-    return st;
+    return st ? st : check_kernel_err(s);
 }
 
 gfb_status gfb_advance_profiled(gfb_solver* s, int32_t n_steps, double* ms_element, double* ms_node,
@@ -2158,6 +2179,29 @@ gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
     info->cells_per_group = use_col_kernel(s) ? s->col_epb : 0;
     info->force_refresh = s->refresh;
     info->half_v = s->half_v ? 1 : 0;
+    info->elem_variant = use_col_kernel(s) ? s->col_variant : -1;
+    info->n_elem_variants = col_kernel_eligible(s) ? s->n_col_variants : 0;
+    return GFB_OK;
+}
+
+gfb_status gfb_select_element_kernel(gfb_solver* s, int32_t variant) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (!col_kernel_eligible(s)) return fail(GFB_ERR_UNSUPPORTED, "this solver has one element kernel");
+    if (variant < -1 || variant >= s->n_col_variants)
+        return fail(GFB_ERR_INVALID, "element kernel variant out of range");
+    gfb_status st;
+    CU(cudaStreamSynchronize(s->stream));
+    s->point_kernel = variant < 0;
+    s->col_variant = variant < 0 ? 0 : variant;
+    if ((st = dispatch<float, ColGridOp>(s->ng, s->nfld, s))) return st;
+    // the next step evaluates the force in full with the new kernel, from
+    // the predicted displacement rewritten in full (between full
+    // evaluations the node pass leaves its increment there)
+    if (s->refresh > 1 && (st = launch_predict(s))) return st;
+    if (s->gexec) {
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
     return GFB_OK;
 }
 
@@ -2165,7 +2209,7 @@ gfb_status gfb_synchronize(gfb_solver* s) {
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     CU(cudaSetDevice(s->device));
     CU(cudaStreamSynchronize(s->stream));
-    return GFB_OK;
+    return check_kernel_err(s);
 }
 
 gfb_status gfb_current_step(const gfb_solver* s, int32_t* step) {

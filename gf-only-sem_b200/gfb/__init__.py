@@ -96,6 +96,8 @@ class Info(C.Structure):
         ("cells_per_group", C.c_int32),
         ("force_refresh", C.c_int32),
         ("half_v", C.c_int32),
+        ("elem_variant", C.c_int32),
+        ("n_elem_variants", C.c_int32),
     ]
 
 
@@ -151,6 +153,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.gfb_create_sources.argtypes = [C.POINTER(Mesh), C.POINTER(Config), C.c_int32, C.POINTER(Source), C.c_int32,
                                        _ip, _ip, C.POINTER(C.c_void_p)]
     lib.gfb_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
+    lib.gfb_select_element_kernel.argtypes = [C.c_void_p, C.c_int32]
     lib.gfb_current_step.argtypes = [C.c_void_p, _ip]
     lib.gfb_get_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
     lib.gfb_set_state.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp, _dp]
@@ -167,6 +170,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
         "gfb_create_batch", "gfb_checkpoint_size", "gfb_checkpoint_save", "gfb_checkpoint_load",
         "gfb_rec_nodes", "gfb_read_green", "gfb_read_record_f32", "gfb_create_sources",
+        "gfb_select_element_kernel",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -343,6 +347,11 @@ class Solver:
         i = Info()
         _check(self.lib.gfb_get_info(self.h, C.byref(i)))
         return {name: getattr(i, name) for name, _ in Info._fields_}
+
+    def select_element_kernel(self, variant: int):
+        """Use element-kernel variant `variant` from the next step on (-1: the
+        thread-per-point kernel; 0..n_elem_variants-1: the line kernel's)."""
+        _check(self.lib.gfb_select_element_kernel(self.h, int(variant)))
 
     def synchronize(self):
         _check(self.lib.gfb_synchronize(self.h))

@@ -43,6 +43,7 @@ def _bind(lib):
     lib.gfb_layer_pack.argtypes = [i32, f32p, C.POINTER(C.c_uint16)]
     lib.gfb_layer_attach.argtypes = [vp, C.POINTER(LayerDesc), C.POINTER(C.c_uint16), f32p, C.c_double]
     lib.gfb_layer_status.argtypes = [vp, C.POINTER(C.c_int32), dp]
+    lib.gfb_layer_set_gains.argtypes = [vp, i32, f32p]
     lib.gfb_trainer_create.argtypes = [i32, i64, i32, u64, C.POINTER(vp)]
     lib.gfb_trainer_destroy.argtypes = [vp]
     lib.gfb_trainer_collect.argtypes = [vp, vp, vp, C.POINTER(C.c_int32), C.POINTER(LayerDesc), i32, i32, i32]
@@ -53,7 +54,8 @@ def _bind(lib):
     lib.gfb_trainer_get_params.argtypes = [vp, f32p, f32p]
     lib.gfb_trainer_set_params.argtypes = [vp, f32p]
     lib.gfb_trainer_evaluate.argtypes = [vp, dp]
-    for n in ("gfb_layer_pack", "gfb_layer_attach", "gfb_layer_status", "gfb_trainer_create", "gfb_trainer_destroy",
+    for n in ("gfb_layer_pack", "gfb_layer_attach", "gfb_layer_status", "gfb_layer_set_gains",
+              "gfb_trainer_create", "gfb_trainer_destroy",
               "gfb_trainer_collect", "gfb_trainer_samples", "gfb_trainer_set_scales", "gfb_trainer_fit",
               "gfb_trainer_gradient", "gfb_trainer_get_params", "gfb_trainer_set_params", "gfb_trainer_evaluate"):
         getattr(lib, n).restype = C.c_int
@@ -291,6 +293,13 @@ def attach(solver: Solver, layer: Layer, params: np.ndarray, scales: np.ndarray,
     solver._layer_keep = (layer, w, s)
 
 
+def set_gains(solver: Solver, gains: np.ndarray):
+    """Damping gains [n_net][3] of the attached layer (network, face axis)."""
+    lib = _bind(load_library())
+    g = np.ascontiguousarray(gains, dtype=np.float32)
+    _check(lib.gfb_layer_set_gains(solver.h, int(g.shape[0]), _ptr(g, C.c_float)))
+
+
 def status(solver: Solver):
     lib = _bind(load_library())
     a = C.c_int32()
@@ -348,3 +357,182 @@ def reflection_error(thin: dict, thin_snaps: dict, thick, thick_snaps: dict, shi
     b = ub[:, pick]
     n = min(a.shape[0], b.shape[0])
     return float(np.linalg.norm(a[:n] - b[:n]) / max(np.linalg.norm(b[:n]), 1e-300))
+
+
+# ---------------------------------------------------------------------------
+# closed loop: whole runs of the thin domain against the thick reference
+# ---------------------------------------------------------------------------
+
+def run_domain(prob: dict, params: Optional[np.ndarray] = None, scales: Optional[np.ndarray] = None,
+               gains: Optional[np.ndarray] = None, scale_mult: float = 1.0, dirs=(0, 1, 2), device: int = 0,
+               n_steps: Optional[int] = None, threshold: float = 0.05, chunk: int = 200, planes=None):
+    """Step prob (FP32, wavefields ``dirs``; with the learned layer when
+    ``params`` are given: output scale times ``scale_mult``, damping gains
+    ``gains``, layer nodes on the depth ``planes``) and return
+    ({field: {"u": float32 [n_snap][n_rec][nn][3]}}, device ms per step,
+    layer status or None)."""
+    n_steps = int(n_steps or prob["nsteps"])
+    s = Solver(prob, dirs=list(dirs), precision=FP32, device=device, record_slots=16, flags=FLAG_RECORD_F32)
+    try:
+        if params is not None:
+            sc = np.array(scales, dtype=np.float32)
+            sc[3] *= scale_mult
+            layer = Layer(prob, planes)
+            attach(s, layer, params, sc, threshold=threshold)
+            if gains is not None:
+                set_gains(s, gains)
+        us = {f: [] for f in range(len(dirs))}
+        ms, done = 0.0, 0
+        while done < n_steps:
+            k = min(chunk, n_steps - done)
+            ms += s.advance_timed(k)
+            while s.pending() > 0:
+                for f in range(len(dirs)):
+                    u = np.empty((s.n_rec, s.nn, 3), dtype=np.float32)
+                    s.read_record(f, release=f == len(dirs) - 1, out={"u": u})
+                    us[f].append(u)
+            done += k
+        st = status(s) if params is not None else None
+    finally:
+        s.close()
+    return {f: {"u": np.stack(us[f])} for f in us}, ms / max(n_steps, 1), st
+
+
+class LoopCase:
+    """A thin domain, the recorded surface displacement of its thick-C-PML
+    reference run (the target of the closed-loop stage), and a solver of the
+    thin domain kept for repeated runs: restored to its step-0 checkpoint
+    and given a freshly attached layer before each."""
+
+    def __init__(self, thin: dict, keys: np.ndarray, ref: dict, shift: float, dirs=(0, 1, 2), device: int = 0):
+        self.thin, self.shift, self.dirs, self.device = thin, shift, tuple(dirs), device
+        ka = surface_keys(thin, shift)
+        idx = {tuple(k): i for i, k in enumerate(keys)}
+        self.sel = np.array([i for i, k in enumerate(ka) if tuple(k) in idx], dtype=np.int64)
+        if self.sel.size == 0:
+            raise ValueError("no common recording cells")
+        pick = np.array([idx[tuple(ka[i])] for i in self.sel], dtype=np.int64)
+        self.ref = {f: np.asarray(ref[f]["u"])[:, pick] for f in ref}
+        self._solver, self._blob, self._layers, self._plain = None, None, {}, None
+
+    def _layer(self, planes):
+        key = None if planes is None else tuple(planes)
+        if key not in self._layers:
+            self._layers[key] = Layer(self.thin, planes)
+        return self._layers[key]
+
+    def _errors(self, snaps) -> list:
+        out = []
+        for f, ref in self.ref.items():
+            a = np.asarray(snaps[f]["u"])[:, self.sel]
+            n = min(a.shape[0], ref.shape[0])
+            out.append(float(np.linalg.norm(a[:n] - ref[:n]) / max(np.linalg.norm(ref[:n]), 1e-300)))
+        return out
+
+    def errors(self, params=None, scales=None, gains=None, scale_mult: float = 1.0, planes=None) -> list:
+        """Reflection error of each wavefield with the given layer (none when
+        params is None)."""
+        if params is None:
+            if self._plain is None:
+                rec, _, _ = run_domain(self.thin, dirs=self.dirs, device=self.device)
+                self._plain = self._errors(rec)
+            return list(self._plain)
+        if self._solver is None:
+            s = Solver(self.thin, dirs=list(self.dirs), precision=FP32, device=self.device, record_slots=16,
+                       flags=FLAG_RECORD_F32)
+            attach(s, self._layer(None), np.zeros_like(params), np.ones(4, dtype=np.float32))
+            self._solver, self._blob = s, s.checkpoint()
+        s = self._solver
+        s.restore(self._blob)
+        sc = np.array(scales, dtype=np.float32)
+        sc[3] *= scale_mult
+        attach(s, self._layer(planes), params, sc)
+        if gains is not None:
+            set_gains(s, gains)
+        n_steps, nf = int(self.thin["nsteps"]), len(self.dirs)
+        us = {f: [] for f in range(nf)}
+        done = 0
+        while done < n_steps:
+            k = min(200, n_steps - done)
+            s.advance(k)
+            s.synchronize()
+            while s.pending() > 0:
+                for f in range(nf):
+                    u = np.empty((s.n_rec, s.nn, 3), dtype=np.float32)
+                    s.read_record(f, release=f == nf - 1, out={"u": u})
+                    us[f].append(u)
+            done += k
+        return self._errors({f: {"u": np.stack(us[f])} for f in us})
+
+    def close(self):
+        if self._solver is not None:
+            self._solver.close()
+            self._solver = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def loop_case(p: PairSpec, dirs=(0, 1, 2), device: int = 0) -> LoopCase:
+    thick = build_domain(p, p.n_thick, p.dt)
+    ref, _, _ = run_domain(thick, dirs=dirs, device=device)
+    keys, dt = surface_keys(thick), thick["dt"]
+    del thick
+    return LoopCase(build_domain(p, p.n_thin, dt), keys, ref, (p.n_thick - p.n_thin) * p.d, dirs, device)
+
+
+def case_errors(case: LoopCase, params=None, scales=None, gains=None, scale_mult: float = 1.0,
+                device: int = 0, planes=None) -> list:
+    """Reflection error of each wavefield of one case with the given layer
+    (none when params is None)."""
+    return case.errors(params, scales, gains, scale_mult, planes)
+
+
+def loop_error(cases, params=None, scales=None, gains=None, scale_mult: float = 1.0, device: int = 0,
+               planes=None) -> float:
+    """RMS reflection error over the cases and their wavefields."""
+    e = [x for c in cases for x in c.errors(params, scales, gains, scale_mult, planes)]
+    return float(np.sqrt(np.mean(np.square(e))))
+
+
+LOG_GAIN_BOUND = 6.0  # gains within e^-6 .. e^6 (the kernel caps the damping at m/dt anyway)
+
+
+def fit_gains(cases, params: np.ndarray, scales: np.ndarray, nets=None, step: float = 1.0,
+              min_step: float = 0.125, max_evals: int = 120, device: int = 0, planes=None):
+    """Closed-loop stage of training: the damping gains [n_net][3] (one per
+    network and face axis) that minimise the reflection error of whole runs
+    of the training cases with the given networks, by coordinate search on
+    log-gains (steps +-step, halved when a sweep brings no improvement,
+    down to min_step).  ``nets``: the networks whose gains are fitted
+    (default: those with nodes in the first case's layer; ``planes`` as in
+    layer_nodes).  Returns (gains, error, history of (evaluations, error))."""
+    n_net = params.shape[0]
+    if nets is None:
+        nets = sorted(set(int(k) for k in Layer(cases[0].thin, planes).net))
+    lg = np.zeros((n_net, 3))
+    best = loop_error(cases, params, scales, np.exp(lg), 1.0, device, planes)
+    evals, hist = 1, [(1, best)]
+    while step >= min_step and evals < max_evals:
+        improved = False
+        for k in nets:
+            for j in range(3):
+                for sgn in (1.0, -1.0):
+                    if evals >= max_evals:
+                        break
+                    trial = lg.copy()
+                    trial[k, j] = np.clip(trial[k, j] + sgn * step, -LOG_GAIN_BOUND, LOG_GAIN_BOUND)
+                    if trial[k, j] == lg[k, j]:
+                        continue
+                    e = loop_error(cases, params, scales, np.exp(trial), 1.0, device, planes)
+                    evals += 1
+                    if e < best:
+                        best, lg, improved = e, trial, True
+                        hist.append((evals, best))
+                        break
+        if not improved:
+            step *= 0.5
+    return np.exp(lg).astype(np.float32), best, hist

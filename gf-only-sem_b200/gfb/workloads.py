@@ -45,6 +45,9 @@ WORKLOADS = {
     "deformed_128x128x64": dict(nx=128, ny=128, nz=64, d=200.0, pml=5, seed=3, src=(12800.0, 12800.0, 2000.0),
                                 nsteps=6000, stride=10, depth=200.0, jitter=0.1, topo=(8, 300.0), corr=150.0,
                                 pert=0.1, tile=16),
+    "deformed_64x64x32": dict(nx=64, ny=64, nz=32, d=200.0, pml=5, seed=3, src=(6400.0, 6400.0, 2000.0),
+                              nsteps=3000, stride=10, depth=200.0, jitter=0.1, topo=(8, 300.0), corr=150.0,
+                              pert=0.1, tile=16),
     "deformed_32x32x16": dict(nx=32, ny=32, nz=16, d=200.0, pml=5, seed=3, src=(3200.0, 3200.0, 1400.0),
                               nsteps=1500, stride=10, depth=200.0, jitter=0.1, topo=(8, 300.0), corr=150.0,
                               pert=0.1, tile=8),

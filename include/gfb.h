@@ -257,9 +257,20 @@ typedef struct gfb_info {
     int32_t cells_per_group; /* cells per block iteration of the line kernel (0 otherwise)  */
     int32_t force_refresh;   /* steps between full element-force evaluations (1: every step) */
     int32_t half_v;          /* 1: plain nodes keep the half-step velocity, no acceleration */
+    int32_t elem_variant;    /* FP32 element kernel in use: -1 thread-per-point; line kernel
+                                with 0 the default cells per group, 1 fewer, 2 more           */
+    int32_t n_elem_variants; /* line-kernel variants built for this ngll / field count
+                                (0: the solver has one element kernel)                        */
 } gfb_info;
 
 gfb_status gfb_get_info(const gfb_solver* solver, gfb_info* info);
+
+/* Use element-kernel variant `variant` (as in gfb_info.elem_variant) from
+ * the next step on, in place of the autotuner's or the default choice; the
+ * next step evaluates the element force in full.  GFB_ERR_UNSUPPORTED when
+ * the solver has one element kernel (FP64, per-cell C-PML, fused node
+ * update); GFB_ERR_INVALID for a variant outside [-1, n_elem_variants). */
+gfb_status gfb_select_element_kernel(gfb_solver* solver, int32_t variant);
 
 /* Wait for all queued work. */
 gfb_status gfb_synchronize(gfb_solver* solver);
@@ -437,6 +448,12 @@ gfb_status gfb_layer_pack(int32_t n_net, const float* params, uint16_t* weights)
  * threshold = fallback limit of the monitored residual. */
 gfb_status gfb_layer_attach(gfb_solver* solver, const gfb_layer* layer, const uint16_t* weights,
                             const float* scales, double threshold);
+
+/* Damping gains [n_net][3] (network, face axis; >= 0, all 1 at attach): the
+ * dashpot coefficient of axis j at a node of network k is
+ * gains[k][j] * (s_c / s_v) * sigma_j.  The closed-loop stage of training
+ * fits them to the reflection error of whole runs. */
+gfb_status gfb_layer_set_gains(gfb_solver* solver, int32_t n_net, const float* gains);
 
 /* Whether the correction is still applied, and the monitored residual. */
 gfb_status gfb_layer_status(gfb_solver* solver, int32_t* active, double* residual);

@@ -219,10 +219,13 @@ def gl_split(p):
 
 
 def test_trained_layer_reduces_reflection_against_thick_cpml():
-    """End to end on small models: collect replays of two seeded pairs, fit,
-    then the reflection error of the thin domain (one-element C-PML) with the
-    trained layer against the 10-element C-PML reference run, on a held-out model,
-    is well below that of the same thin domain without the layer."""
+    """End to end on small models: collect replays of two seeded pairs and
+    fit the networks; fit the damping gains in closed loop on two further
+    training models; then on a held-out model the reflection error of the
+    thin domain (one-element C-PML) against the 10-element C-PML reference
+    run is well below that of the thin domain without the layer, and the
+    layer with its closed-loop gains beats the untrained layer (constant
+    damping softplus(0) on every axis, unit gains)."""
     def pair(seed, steps):
         r = np.random.default_rng(seed)
         return gl.PairSpec(ni=6, nj=6, nk=4, d=500.0, seed=seed, f0=float(r.uniform(0.8, 1.2)),
@@ -239,24 +242,22 @@ def test_trained_layer_reduces_reflection_against_thick_cpml():
     assert loss[-1] < base
     params, scales = tr.params()
     tr.close()
-    p = pair(99, 500)
-    thin, thick, _ = gl.build_pair(p)
-    shift = (p.n_thick - p.n_thin) * p.d
+    zero = params * 0.0
 
-    def run(prob, learned):
-        s = gfb.Solver(prob, dirs=[0], precision=gfb.FP32, record_slots=64)
-        if learned:
-            gl.attach(s, gl.Layer(prob), params, scales, threshold=0.05)
-        s.advance(p.nsteps)
-        out = s.drain()[0]
-        st = gl.status(s) if learned else None
-        s.close()
-        return out, st
+    cases = [gl.loop_case(pair(40 + k, 400), dirs=(0, 1, 2)) for k in range(2)]
+    gains, e_fit, hist = gl.fit_gains(cases, zero, scales, max_evals=30)
+    assert e_fit < hist[0][1]  # the closed loop lowered the training error
+    assert gains.shape == (n_net, 3) and np.all(gains > 0)
 
-    thick_rec, _ = run(thick, False)
-    plain, _ = run(thin, False)
-    learned, st = run(thin, True)
+    test = gl.loop_case(pair(99, 500), dirs=(0, 1, 2))
+    e_plain = gl.loop_error([test])
+    e_replay = gl.loop_error([test], params, scales)
+    e_untrained = gl.loop_error([test], zero, scales)
+    e_learned = gl.loop_error([test], zero, scales, gains)
+    rec, _, st = gl.run_domain(test.thin, zero, scales, gains)
     assert st[0]  # still active: no fallback was needed
-    e_plain = gl.reflection_error(thin, plain, thick, thick_rec, shift)
-    e_learned = gl.reflection_error(thin, learned, thick, thick_rec, shift)
+    print(f"held-out: no layer {e_plain:.4f}, untrained {e_untrained:.4f}, replay-trained {e_replay:.4f}, "
+          f"closed-loop gains {e_learned:.4f} (training {hist[0][1]:.4f} -> {e_fit:.4f}), gains {gains[sorted(set(gl.Layer(test.thin).net))]}")
+    assert e_replay < 0.7 * e_plain, (e_replay, e_plain)
     assert e_learned < 0.7 * e_plain, (e_learned, e_plain)
+    assert e_learned < e_untrained, (e_learned, e_untrained)

@@ -276,6 +276,63 @@ def test_fp32_line_and_point_kernels_agree():
             assert rel_l2(line[d][k], point[d][k]) < 1e-5
 
 
+@pytest.mark.parametrize("dirs", [[2], [0, 1], [0, 1, 2]])
+def test_fp32_line_kernel_variants_agree(dirs):
+    """Every variant of the line kernel at order 4 (cells per group default,
+    fewer, more; the default with its stages filled by bulk copies): the same
+    sums in the same order per xi-line, so the traces are bit-identical to
+    the default variant's, and within 1e-4 of the oracle; and kernels
+    switched between steps."""
+    n = 120
+    prob = layered_problem(nsteps=n)
+    runs = {}
+    s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
+    n_var = s.info()["n_elem_variants"]
+    s.close()
+    assert n_var == 4
+    for v in range(n_var):
+        s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
+        s.select_element_kernel(v)
+        assert s.info()["elem_variant"] == v
+        s.advance(n)
+        runs[v] = s.drain()
+        s.close()
+    for f, d in enumerate(dirs):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(runs[0][f], ref, FP32_TOL, f"line kernel field {d}")
+        for v in range(1, n_var):
+            for k in ("strain", "u", "v", "a"):
+                np.testing.assert_array_equal(runs[v][f][k], runs[0][f][k], err_msg=f"variant {v} {k}")
+    # switching kernels between steps (the next step evaluates in full, off
+    # the 100-step schedule): still within 1e-4 of the oracle
+    s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
+    s.advance(n // 3)
+    s.select_element_kernel(3)
+    s.advance(n // 3)
+    s.select_element_kernel(-1)
+    assert s.info()["elem_variant"] == -1
+    s.advance(n - 2 * (n // 3))
+    mixed = s.drain()
+    s.close()
+    for f, d in enumerate(dirs):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(mixed[f], ref, FP32_TOL, f"switched kernels field {d}")
+
+
+def test_element_kernel_selection_is_checked():
+    prob = layered_problem(nsteps=10)
+    s = gfb.Solver(prob, dirs=[0], precision=gfb.FP32)
+    for bad in (-2, s.info()["n_elem_variants"]):
+        with pytest.raises(gfb.GfbError, match="out of range"):
+            s.select_element_kernel(bad)
+    s.close()
+    s = gfb.Solver(prob, dirs=[0], precision=gfb.FP64)
+    assert s.info()["n_elem_variants"] == 0 and s.info()["elem_variant"] == -1
+    with pytest.raises(gfb.GfbError, match="one element kernel"):
+        s.select_element_kernel(0)
+    s.close()
+
+
 @pytest.mark.parametrize("order,dirs", [(2, [1]), (3, [0, 2]), (5, [0, 1, 2]), (4, [2])])
 def test_fp32_line_kernel_orders_and_field_counts(order, dirs):
     """Every (order, wavefield count) shape of the line kernel: its cells per
