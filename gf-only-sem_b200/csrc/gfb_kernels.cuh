@@ -992,8 +992,27 @@ __global__ void __launch_bounds__(PipeShape<Real, NG, NFLD>::THREADS, (sizeof(Re
 // the kernel parameters (constant bank); those indexed by the thread's own j
 // and k are kept in registers.
 //
+// XCH (line owners): instead of every thread reading the five eta and five
+// zeta neighbours of each of its points (30 shared loads per point for the
+// gradient, 30 for the divergence), the thread with column (j, k) also owns
+// the eta line (i = j, k) and the zeta line (i = k, j) of its (cell,
+// wavefield): it reads the line, contracts it with D in registers and
+// writes the derivative back in place, so a point costs one shared load per
+// direction and component afterwards.  Phases per group: own points'
+// displacement into both arrays | line contractions | gradient, stress and
+// fluxes (the eta and zeta fluxes replace the derivatives in place) | line
+// contractions of the fluxes | divergence and assembly; four barriers instead
+// of two, and 40 % fewer shared-memory wavefronts.  The arrays' point layout
+// (PIE, PIZ) and slot stride SP put a warp's own-point accesses and its
+// line accesses in distinct banks.  The eta and zeta sums of the divergence
+// are added in another order than in the default layout, so the two agree
+// to rounding, not bit for bit.
+//
 // Pipelining: the geometry of the next group and the node table of the one
-// after are cp.async copies into rotating shared stages; the next group's
+// after are bulk copies (TMA engine, one per cell, issued by one thread and
+// completing on a per-stage mbarrier) into rotating shared stages; the
+// writes bypass the LSU pipe that the shared-memory exchange keeps busy,
+// which 16-byte cp.async by every thread did not; the next group's
 // predicted-displacement vectors are register loads issued one group ahead,
 // this group's old force vectors are prefetched into L2 at the start of the
 // group and loaded into registers once its gradient phase is done.
@@ -1005,7 +1024,10 @@ __host__ __device__ constexpr int col_default_epb(int ng, int nfld) {
     return (150 / (nfld * ng * ng)) > 0 ? 150 / (nfld * ng * ng) : 1;
 }
 
-template <int NG, int NFLD, int EPB_ = col_default_epb(NG, NFLD)>
+// XCH: the eta and zeta contractions done by line owners (see
+// elem_col_kernel) in two [3][GR][SP] arrays laid out point (i, j, k) ->
+// PI*i + NG*j + k with PI = PIE (eta array) or PIZ (zeta array).
+template <int NG, int NFLD, int EPB_ = col_default_epb(NG, NFLD), bool XCH = false>
 struct ColShape {
     static constexpr int NN = NG * NG * NG;
     static constexpr int NG2 = NG * NG;
@@ -1013,13 +1035,19 @@ struct ColShape {
     static constexpr int GR = EPB * NFLD;                 // (cell, wavefield) lines per group
     static constexpr int ACTIVE = GR * NG2;               // threads with work
     static constexpr int THREADS = (ACTIVE + 31) / 32 * 32;
-    static constexpr int SP = NN + ((NG2 - NN) % 32 + 32) % 32;  // >= NN, == NG2 (mod 32)
+    // at NG = 5 (PIE, PIZ, SP) = (37, 33, 185): the own-point accesses and
+    // the eta- (zeta-) line accesses of a warp fall in distinct banks
+    static constexpr int PIE = NG2 + 12, PIZ = NG2 + 8;
+    static constexpr int SP = XCH ? NG * PIE : NN + ((NG2 - NN) % 32 + 32) % 32;  // >= NN, == NG2 (mod 32)
     static constexpr int GEO_B = 12 * NN * 4;
     static constexpr int GEO_W = GEO_B / 4;
     static constexpr int GEO_SLOT = GEO_B + 4 * (((24 - GEO_W) % 32 + 32) % 32 / 4 * 4);
     static constexpr int IB_B = ib_row_words(NN) * 4;
     static constexpr int ARR = 3 * GR * SP;               // floats of one [3][GR][SP] array
-    static constexpr int SMEM = 2 * EPB * GEO_SLOT + 3 * EPB * IB_B + (3 * ARR + 64) * 4;
+    static constexpr int N_ARR = XCH ? 2 : 3;
+    // dynamic shared memory without the per-model values (col_model_smem)
+    static constexpr int SMEM = 2 * EPB * GEO_SLOT + 3 * EPB * IB_B + (N_ARR * ARR + 64) * 4;
+    static constexpr int MIN_BLOCKS = THREADS <= 160 ? 3 : 2;
     static_assert(GEO_B % 16 == 0 && GEO_SLOT % 16 == 0 && IB_B % 16 == 0, "16-byte copies");
 };
 
@@ -1047,13 +1075,14 @@ struct ColArgs {
     float D[36];                   // D[i*NG+s], read with compile-time indices only
 };
 
-// TMA: the geometry and node-table stages are filled by bulk copies (one per
-// cell, issued by one thread, completing on a per-stage mbarrier) instead of
-// 16-byte cp.async by every thread.
-template <int NG, int NFLD, int EPB_, bool TMA = false>
-__global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<NG, NFLD, EPB_>::THREADS <= 160 ? 3 : 2))
+// Shared bytes of the per-model values of elem_col_kernel: source time
+// function values [n_model][n_set], live and full-force flags [n_model].
+__host__ __device__ constexpr int col_model_smem(int n_model, int n_set) { return (n_model * n_set + 2 * n_model) * 4; }
+
+template <int NG, int NFLD, int EPB_, bool XCH = false>
+__global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_, XCH>::THREADS, ColShape<NG, NFLD, EPB_, XCH>::MIN_BLOCKS)
     elem_col_kernel(ColArgs A) {
-    using S = ColShape<NG, NFLD, EPB_>;
+    using S = ColShape<NG, NFLD, EPB_, XCH>;
     constexpr int NN = S::NN, NG2 = S::NG2, EPB = S::EPB, GR = S::GR, SP = S::SP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* gbase = smem_raw;
@@ -1061,7 +1090,11 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     float* us = reinterpret_cast<float*>(ibase + 3 * EPB * S::IB_B);  // [3][GR][SP] displacement
     float* fe = us + S::ARR;                                          // [3][GR][SP] eta flux
     float* fz = fe + S::ARR;                                          // [3][GR][SP] zeta flux
-    float* sD = fz + S::ARR;
+    float* sD = us + S::N_ARR * S::ARR;
+    // XCH: [3][GR][SP] eta and zeta arrays (u, then its derivative, the
+    // flux, then the flux's contraction, each in place)
+    float* xe = us;
+    float* xz = us + S::ARR;
 
     // cells of this colour that still step (several models: the cells past
     // the last one of a live model belong to finished models)
@@ -1076,9 +1109,10 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     int dir, fs;
     field_source<NFLD>(A.dir, A.fset, fld, dir, fs);
     // per-model step flags and source values of this step, read once per block
-    __shared__ float s_stf[kMaxModels];
-    __shared__ int s_live[kMaxModels];
-    __shared__ int s_direct[kMaxModels];
+    // (in the dynamic shared memory after sD: col_model_smem bytes)
+    float* s_stf = sD + 64;
+    int* s_live = reinterpret_cast<int*>(s_stf + A.n_model * A.n_set);
+    int* s_direct = s_live + A.n_model;
     for (int m = tid; m < A.n_model * A.n_set; m += S::THREADS) s_stf[m] = A.mstf[m];
     for (int m = tid; m < A.n_model; m += S::THREADS) {
         s_live[m] = A.mlive[m];
@@ -1100,26 +1134,6 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
     };
     auto ib_of = [&](int st, int c) -> const uint32_t* {
         return reinterpret_cast<const uint32_t*>(ibase + (st * EPB + c) * S::IB_B);
-    };
-    auto issue_ib = [&](int grp, int st) {
-        constexpr int CI = S::IB_B / 16;
-        for (int q = tid; q < EPB * CI; q += S::THREADS) {
-            const int c = q / CI, r = q - c * CI;
-            const int e = A.e_begin + grp * EPB + c;
-            if (e < e_end)
-                cp_async16(ibase + (st * EPB + c) * S::IB_B + r * 16,
-                           reinterpret_cast<const unsigned char*>(A.ibool_padded) + (size_t)e * S::IB_B + r * 16);
-        }
-    };
-    auto issue_geo = [&](int grp, int st) {
-        constexpr int CG = S::GEO_B / 16;
-        for (int q = tid; q < EPB * CG; q += S::THREADS) {
-            const int c = q / CG, r = q - c * CG;
-            const int e = A.e_begin + grp * EPB + c;
-            if (e < e_end)
-                cp_async16(gbase + (st * EPB + c) * S::GEO_SLOT + r * 16,
-                           reinterpret_cast<const unsigned char*>(A.geom) + (size_t)e * S::GEO_B + r * 16);
-        }
     };
     // node words of this thread's line of group grp (node table in stage st)
     auto line_nodes = [&](int grp, int st, uint32_t (&w)[NG]) -> bool {
@@ -1169,40 +1183,32 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
 
     const int G = gridDim.x;
     const int grp0 = blockIdx.x;
-    if constexpr (TMA) {
-        if (tid == 0) {
-            for (int b = 0; b < 5; ++b) mbar_init(&s_bar[b], 1);
-            mbar_init_fence();
-        }
-        __syncthreads();
-        if (grp0 < n_groups) tma_ib(grp0, 0);
-        const bool bad = grp0 < n_groups && !mbar_wait(&s_bar[2], 0);
-        if (__syncthreads_or(bad)) {
-            give_up(2, 0, -1, 0);
-            return;
-        }
-    } else {
-        if (grp0 < n_groups) issue_ib(grp0, 0);
-        cp_async_commit();
-        cp_async_wait_all();
-        __syncthreads();
+    if (tid == 0) {
+        for (int b = 0; b < 5; ++b) mbar_init(&s_bar[b], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (grp0 < n_groups) tma_ib(grp0, 0);
+    if (__syncthreads_or(grp0 < n_groups && !mbar_wait(&s_bar[2], 0))) {
+        give_up(2, 0, -1, 0);
+        return;
     }
     uint32_t nw[NG];
     float4 pre[NG];
     bool pre_ok = line_nodes(grp0, 0, nw);
     load_vectors(nw, pre_ok, pre);
-    if constexpr (TMA) {
-        if (grp0 < n_groups) tma_geo(grp0, 0);
-        if (grp0 + G < n_groups) tma_ib(grp0 + G, 1);
-    } else {
-        if (grp0 < n_groups) issue_geo(grp0, 0);
-        if (grp0 + G < n_groups) issue_ib(grp0 + G, 1);
-        cp_async_commit();
-    }
+    if (grp0 < n_groups) tma_geo(grp0, 0);
+    if (grp0 + G < n_groups) tma_ib(grp0 + G, 1);
 
     const int ubase = line * SP + col;        // + c*GR*SP + i*NG2
     const int ebase = line * SP + col - j * NG;  // + s*NG  (eta line: i*NG2 + s*NG + k)
     const int zbase = line * SP + j * NG;        // + s     (zeta line: i*NG2 + j*NG + s)
+    // XCH: own points (i, j, k) at xown + i*PI; the eta line this thread owns
+    // is (i = j, k = k) of its (cell, wavefield): points xline_e + s*NG; the
+    // zeta line is (i = k, j = j): points xline_z + s
+    const int xown_e = line * SP + j * NG + k, xown_z = xown_e;
+    const int xline_e = line * SP + j * S::PIE + k;
+    const int xline_z = line * SP + k * S::PIZ + j * NG;
 
     int it = 0;
     for (int grp = grp0; grp < n_groups; grp += G, ++it) {
@@ -1221,13 +1227,22 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
             u1[i] = pre[i].y;
             u2[i] = pre[i].z;
             if (act) {
-                us[0 * GR * SP + ubase + i * NG2] = u0[i];
-                us[1 * GR * SP + ubase + i * NG2] = u1[i];
-                us[2 * GR * SP + ubase + i * NG2] = u2[i];
+                if constexpr (XCH) {
+                    xe[0 * GR * SP + xown_e + i * S::PIE] = u0[i];
+                    xe[1 * GR * SP + xown_e + i * S::PIE] = u1[i];
+                    xe[2 * GR * SP + xown_e + i * S::PIE] = u2[i];
+                    xz[0 * GR * SP + xown_z + i * S::PIZ] = u0[i];
+                    xz[1 * GR * SP + xown_z + i * S::PIZ] = u1[i];
+                    xz[2 * GR * SP + xown_z + i * S::PIZ] = u2[i];
+                } else {
+                    us[0 * GR * SP + ubase + i * NG2] = u0[i];
+                    us[1 * GR * SP + ubase + i * NG2] = u1[i];
+                    us[2 * GR * SP + ubase + i * NG2] = u2[i];
+                }
             }
         }
         const int nx = grp + G;
-        if constexpr (TMA) {
+        {
             // stage it&1 holds this group's geometry (use it/2 of that stage),
             // stage (it+1)%3 the next group's node table (use (it+1)/3)
             const unsigned pg = (unsigned)(it >> 1) & 1u, pi = (unsigned)((it + 1) / 3) & 1u;
@@ -1238,15 +1253,9 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                 give_up(it & 1, pg, bi, pi);
                 return;
             }
-            if (nx < n_groups) tma_geo(nx, (it + 1) & 1);
-            if (nx + G < n_groups) tma_ib(nx + G, (it + 2) % 3);
-        } else {
-            cp_async_wait_all();
-            __syncthreads();  // displacement of this group, its geometry, the next node table
-            if (nx < n_groups) issue_geo(nx, (it + 1) & 1);
-            if (nx + G < n_groups) issue_ib(nx + G, (it + 2) % 3);
-            cp_async_commit();
         }
+        if (nx < n_groups) tma_geo(nx, (it + 1) & 1);
+        if (nx + G < n_groups) tma_ib(nx + G, (it + 2) % 3);
         // old force vectors of the nodes this colour does not touch first:
         // start their DRAM reads into L2 now, so the loads issued after the
         // flux phase find them there (no registers held meanwhile)
@@ -1263,6 +1272,45 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
         pre_ok = line_nodes(nx, (it + 1) % 3, nw);
         load_vectors(nw, pre_ok, pre);
 
+        // old force of the nodes this colour does not touch first
+        float4 of[NG];
+        auto load_old_force = [&]() {
+#pragma unroll
+            for (int i = 0; i < NG; ++i)
+                of[i] = (act && !(cw[i] & first_bit))
+                            ? *(reinterpret_cast<const float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+        };
+        if constexpr (XCH) {
+            // line owners: d/d-eta along this thread's eta line and d/d-zeta
+            // along its zeta line, in place (the lines of a (cell, wavefield)
+            // are disjoint; the two arrays hold the same displacement)
+            if (act) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    float* le = xe + c * GR * SP + xline_e;
+                    float* lz = xz + c * GR * SP + xline_z;
+                    float ve[NG], vz[NG];
+#pragma unroll
+                    for (int t = 0; t < NG; ++t) {
+                        ve[t] = le[t * NG];
+                        vz[t] = lz[t];
+                    }
+#pragma unroll
+                    for (int s2 = 0; s2 < NG; ++s2) {
+                        float de = 0.f, dz = 0.f;
+#pragma unroll
+                        for (int t = 0; t < NG; ++t) {
+                            de += A.D[s2 * NG + t] * ve[t];
+                            dz += A.D[s2 * NG + t] * vz[t];
+                        }
+                        le[s2 * NG] = de;
+                        lz[s2] = dz;
+                    }
+                }
+            }
+            __syncthreads();  // the eta and zeta derivatives of the whole group
+        }
         // gradient, stress and the three fluxes at each point of the line
         float fx0[NG], fx1[NG], fx2[NG];
         const float* geo = geo_of(it & 1, cl);
@@ -1283,13 +1331,21 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                 gx[1] += Di * u1[s];
                 gx[2] += Di * u2[s];
             }
+            if constexpr (XCH) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float* uc = us + c * GR * SP + i * NG2;
+                for (int c = 0; c < 3; ++c) {
+                    gy[c] = xe[c * GR * SP + xown_e + i * S::PIE];
+                    gz[c] = xz[c * GR * SP + xown_z + i * S::PIZ];
+                }
+            } else {
 #pragma unroll
-                for (int s = 0; s < NG; ++s) {
-                    gy[c] += Dj[s] * uc[ebase + s * NG];
-                    gz[c] += Dk[s] * uc[zbase + s];
+                for (int c = 0; c < 3; ++c) {
+                    const float* uc = us + c * GR * SP + i * NG2;
+#pragma unroll
+                    for (int s = 0; s < NG; ++s) {
+                        gy[c] += Dj[s] * uc[ebase + s * NG];
+                        gz[c] += Dk[s] * uc[zbase + s];
+                    }
                 }
             }
             float st0 = 0.f, st1 = 0.f, st2 = 0.f, st3 = 0.f, st4 = 0.f, st5 = 0.f;
@@ -1314,21 +1370,59 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
             fx0[i] = jw * (st0 * dd[0] + st3 * dd[3] + st4 * dd[6]);
             fx1[i] = jw * (st3 * dd[0] + st1 * dd[3] + st5 * dd[6]);
             fx2[i] = jw * (st4 * dd[0] + st5 * dd[3] + st2 * dd[6]);
-            fe[0 * GR * SP + ubase + i * NG2] = jw * (st0 * dd[1] + st3 * dd[4] + st4 * dd[7]);
-            fe[1 * GR * SP + ubase + i * NG2] = jw * (st3 * dd[1] + st1 * dd[4] + st5 * dd[7]);
-            fe[2 * GR * SP + ubase + i * NG2] = jw * (st4 * dd[1] + st5 * dd[4] + st2 * dd[7]);
-            fz[0 * GR * SP + ubase + i * NG2] = jw * (st0 * dd[2] + st3 * dd[5] + st4 * dd[8]);
-            fz[1 * GR * SP + ubase + i * NG2] = jw * (st3 * dd[2] + st1 * dd[5] + st5 * dd[8]);
-            fz[2 * GR * SP + ubase + i * NG2] = jw * (st4 * dd[2] + st5 * dd[5] + st2 * dd[8]);
+            const float e0 = jw * (st0 * dd[1] + st3 * dd[4] + st4 * dd[7]);
+            const float e1 = jw * (st3 * dd[1] + st1 * dd[4] + st5 * dd[7]);
+            const float e2 = jw * (st4 * dd[1] + st5 * dd[4] + st2 * dd[7]);
+            const float z0 = jw * (st0 * dd[2] + st3 * dd[5] + st4 * dd[8]);
+            const float z1 = jw * (st3 * dd[2] + st1 * dd[5] + st5 * dd[8]);
+            const float z2 = jw * (st4 * dd[2] + st5 * dd[5] + st2 * dd[8]);
+            if constexpr (XCH) {  // own points: the derivatives read above are replaced
+                xe[0 * GR * SP + xown_e + i * S::PIE] = e0;
+                xe[1 * GR * SP + xown_e + i * S::PIE] = e1;
+                xe[2 * GR * SP + xown_e + i * S::PIE] = e2;
+                xz[0 * GR * SP + xown_z + i * S::PIZ] = z0;
+                xz[1 * GR * SP + xown_z + i * S::PIZ] = z1;
+                xz[2 * GR * SP + xown_z + i * S::PIZ] = z2;
+            } else {
+                fe[0 * GR * SP + ubase + i * NG2] = e0;
+                fe[1 * GR * SP + ubase + i * NG2] = e1;
+                fe[2 * GR * SP + ubase + i * NG2] = e2;
+                fz[0 * GR * SP + ubase + i * NG2] = z0;
+                fz[1 * GR * SP + ubase + i * NG2] = z1;
+                fz[2 * GR * SP + ubase + i * NG2] = z2;
+            }
         }
-        // old force of the nodes this colour does not touch first
-        float4 of[NG];
-#pragma unroll
-        for (int i = 0; i < NG; ++i)
-            of[i] = (act && !(cw[i] & first_bit))
-                        ? *(reinterpret_cast<const float4*>(A.force) + (size_t)(cw[i] & kNodeMask) * NFLD + fld)
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
+        load_old_force();
         __syncthreads();  // fluxes of the whole group
+        if constexpr (XCH) {
+            // line owners: the eta (zeta) contraction of the divergence along
+            // this thread's eta (zeta) line, in place
+            if (act) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    float* le = xe + c * GR * SP + xline_e;
+                    float* lz = xz + c * GR * SP + xline_z;
+                    float ve[NG], vz[NG];
+#pragma unroll
+                    for (int t = 0; t < NG; ++t) {
+                        ve[t] = le[t * NG];
+                        vz[t] = lz[t];
+                    }
+#pragma unroll
+                    for (int s2 = 0; s2 < NG; ++s2) {
+                        float de = 0.f, dz = 0.f;
+#pragma unroll
+                        for (int t = 0; t < NG; ++t) {
+                            de += A.D[t * NG + s2] * ve[t];
+                            dz += A.D[t * NG + s2] * vz[t];
+                        }
+                        le[s2 * NG] = de;
+                        lz[s2] = dz;
+                    }
+                }
+            }
+            __syncthreads();  // contractions of the whole group
+        }
         if (act) {
 #pragma unroll
             for (int i = 0; i < NG; ++i) {
@@ -1341,14 +1435,22 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
                     r[1] += Ti * fx1[s];
                     r[2] += Ti * fx2[s];
                 }
+                if constexpr (XCH) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const float* ec = fe + c * GR * SP + i * NG2;
-                    const float* zc = fz + c * GR * SP + i * NG2;
+                    for (int c = 0; c < 3; ++c) {
+                        r[c] += xe[c * GR * SP + xown_e + i * S::PIE];
+                        r[c] += xz[c * GR * SP + xown_z + i * S::PIZ];
+                    }
+                } else {
 #pragma unroll
-                    for (int s = 0; s < NG; ++s) {
-                        r[c] += Tj[s] * ec[ebase + s * NG];
-                        r[c] += Tk[s] * zc[zbase + s];
+                    for (int c = 0; c < 3; ++c) {
+                        const float* ec = fe + c * GR * SP + i * NG2;
+                        const float* zc = fz + c * GR * SP + i * NG2;
+#pragma unroll
+                        for (int s = 0; s < NG; ++s) {
+                            r[c] += Tj[s] * ec[ebase + s * NG];
+                            r[c] += Tk[s] * zc[zbase + s];
+                        }
                     }
                 }
                 r[0] = -r[0];
@@ -1370,7 +1472,6 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_>::THREADS, (ColShape<N
             }
         }
     }
-    cp_async_wait_all();
 }
 
 // Predictor only (start of a run or after a state overwrite).

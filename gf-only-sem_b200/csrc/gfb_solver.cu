@@ -261,7 +261,7 @@ struct gfb_solver {
     uint32_t* ibool_padded = nullptr;  // [cell][NNP] for the pipelined kernel
     int pipe_blocks = 0;               // persistent grid of the element kernel
     int col_blocks = 0;                // persistent grid of the line kernel (FP32)
-    int col_variant = 0;               // cells per group: 0 default, 1 fewer, 2 more
+    int col_variant = 0;               // cells per group: 0 default, 1 fewer, 2 more; 3 default, line owners
     int n_col_variants = 1;
     int col_epb = 0;                   // cells per group of the variant in use
     bool point_kernel = false;         // thread-per-point element kernel on the FP32 path
@@ -584,9 +584,9 @@ bool col_kernel_eligible(const gfb_solver* s) {
 }
 bool use_col_kernel(const gfb_solver* s) { return col_kernel_eligible(s) && !s->point_kernel; }
 
-template <int NG, int NFLD, int EPB, bool TMA = false>
+template <int NG, int NFLD, int EPB, bool XCH = false>
 gfb_status launch_col_e(gfb_solver* s, int c) {
-    using S = gfb::ColShape<NG, NFLD, EPB>;
+    using S = gfb::ColShape<NG, NFLD, EPB, XCH>;
     gfb::ColArgs A;
     A.e_begin = s->colour_begin[c];
     A.e_end = s->colour_begin[c + 1];
@@ -616,21 +616,23 @@ gfb_status launch_col_e(gfb_solver* s, int c) {
     for (int q = 0; q < 36; ++q) A.D[q] = q < NG * NG ? s->dmat_host[q] : 0.f;
     const int blocks = std::max(1, std::min(A.n_groups, s->col_blocks));
     A.err = reinterpret_cast<unsigned*>(s->d_kernel_err);
-    gfb::elem_col_kernel<NG, NFLD, EPB, TMA><<<blocks, S::THREADS, S::SMEM, s->stream>>>(A);
+    const int smem = S::SMEM + gfb::col_model_smem(s->n_model, s->n_set);
+    gfb::elem_col_kernel<NG, NFLD, EPB, XCH><<<blocks, S::THREADS, smem, s->stream>>>(A);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
 }
 
-// Cells-per-group candidates of the line kernel: the default, and at
-// ngll 5 one fewer ("LO") and one more ("HI") step.
+// Candidates of the line kernel: the default cells per group, and at
+// ngll 5 one fewer ("LO") and one more ("HI") step, and the default with
+// the eta/zeta contractions done by line owners (ColShape's XCH).
 constexpr int col_epb_lo(int nfld) { return nfld == 3 ? 1 : (nfld == 2 ? 2 : 4); }
 constexpr int col_epb_hi(int nfld) { return nfld == 3 ? 3 : (nfld == 2 ? 4 : 8); }
 template <int NG, int NFLD>
 struct ColEpb {
     static constexpr int D = gfb::col_default_epb(NG, NFLD);
-    // the fewer / more cells-per-group variants exist for ngll 5 with up to
-    // three wavefields (more would exceed a block's threads)
+    // the other variants exist for ngll 5 with up to three wavefields (more
+    // would exceed a block's threads)
     static constexpr int N = (NG == 5 && NFLD <= 3) ? 4 : 1;
 };
 
@@ -646,13 +648,14 @@ gfb_status launch_col_t(gfb_solver* s, int c) {
 }
 
 // Persistent grid of the line kernel variant EPB: occupancy x SMs.
-template <int NG, int NFLD, int EPB, bool TMA = false>
+template <int NG, int NFLD, int EPB, bool XCH = false>
 gfb_status col_grid(gfb_solver* s, int* blocks) {
-    using C = gfb::ColShape<NG, NFLD, EPB>;
-    auto* fn = gfb::elem_col_kernel<NG, NFLD, EPB, TMA>;
-    CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    using C = gfb::ColShape<NG, NFLD, EPB, XCH>;
+    auto* fn = gfb::elem_col_kernel<NG, NFLD, EPB, XCH>;
+    const int smem = C::SMEM + gfb::col_model_smem(s->n_model, s->n_set);
+    CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0, n_sm = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, C::THREADS, C::SMEM));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, C::THREADS, smem));
     CU(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->device));
     if (per_sm < 1) return fail(GFB_ERR_UNSUPPORTED, "line element kernel does not fit on an SM");
     *blocks = per_sm * n_sm;

@@ -278,11 +278,11 @@ def test_fp32_line_and_point_kernels_agree():
 
 @pytest.mark.parametrize("dirs", [[2], [0, 1], [0, 1, 2]])
 def test_fp32_line_kernel_variants_agree(dirs):
-    """Every variant of the line kernel at order 4 (cells per group default,
-    fewer, more; the default with its stages filled by bulk copies): the same
-    sums in the same order per xi-line, so the traces are bit-identical to
-    the default variant's, and within 1e-4 of the oracle; and kernels
-    switched between steps."""
+    """Every variant of the line kernel at order 4: cells per group default,
+    fewer, more (the same sums in the same order per xi-line, so the traces
+    are bit-identical to the default variant's) and the line-owner exchange
+    (the eta and zeta sums added in another order: within 1e-5); all within
+    1e-4 of the oracle; and kernels switched between steps."""
     n = 120
     prob = layered_problem(nsteps=n)
     runs = {}
@@ -300,9 +300,12 @@ def test_fp32_line_kernel_variants_agree(dirs):
     for f, d in enumerate(dirs):
         ref, _ = oracle_snaps(prob, d, n)
         compare_runs(runs[0][f], ref, FP32_TOL, f"line kernel field {d}")
-        for v in range(1, n_var):
+        compare_runs(runs[3][f], ref, FP32_TOL, f"line-owner exchange field {d}")
+        for v in (1, 2):
             for k in ("strain", "u", "v", "a"):
                 np.testing.assert_array_equal(runs[v][f][k], runs[0][f][k], err_msg=f"variant {v} {k}")
+        for k in ("u", "strain"):
+            assert rel_l2(runs[3][f][k], runs[0][f][k]) < 1e-5
     # switching kernels between steps (the next step evaluates in full, off
     # the 100-step schedule): still within 1e-4 of the oracle
     s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
