@@ -422,8 +422,8 @@ def elem_bytes_per_step(prob, info, n_field, prec):
     """Algorithmic DRAM bytes of one step's element/assembly launches
     (unpadded component bytes; the [node][field][4] layout moves 4/3 of the
     gather/force bytes, visible in the ncu traffic).  With the force updated
-    by increments (99 of 100 steps) every touch of a node reads and writes
-    its force."""
+    by increments (all but one step in the refresh period) every touch of a
+    node reads and writes its force."""
     nn = 125
     P = prob["n_cell"] * nn
     G = prob["n_node"]
@@ -444,8 +444,9 @@ def elem_bytes_per_step(prob, info, n_field, prec):
 
 def node_bytes_per_step(prob, info, n_field, prec):
     """Algorithmic DRAM bytes of one step's node passes: per node and value
-    u and v read and written (FP64), the acceleration read and written
-    (Real; not at plain nodes in the half-step velocity form), the assembled
+    u and v read and written (FP64; at plain nodes in the half-step velocity
+    form the velocity is the half-step one in FP32 and there is no
+    acceleration), the acceleration read and written (Real), the assembled
     force read and the next predicted displacement (or its increment)
     written (Real, unpadded), the mass (1/m in FP32); plus the node-form
     C-PML coefficients, previous field and memory of the live axes."""
@@ -453,9 +454,9 @@ def node_bytes_per_step(prob, info, n_field, prec):
     F = 3 * n_field
     n_pml = info["n_pml_node"]
     n_plain = prob["n_node"] - n_pml
-    acc = 0 if info.get("half_v") else 2 * sr
+    state = 16 + 8 if info.get("half_v") else 16 + 16 + 2 * sr   # u (+ w | v, a) read and written
     mass = 4 if prec == 1 else 8
-    base = n_plain * (F * (32 + acc + 2 * sr) + mass) + n_pml * (F * (32 + 4 * sr) + mass)
+    base = n_plain * (F * (state + 2 * sr) + mass) + n_pml * (F * (32 + 4 * sr) + mass)
     if n_pml > 0:                                    # node-form C-PML in this kernel
         n_live, live = node_pml_live_axes(prob)
         base += n_live * (14 * sr + F * sr * 2) + live * F * sr * 2
@@ -868,10 +869,13 @@ def run_accuracy(args):
     rs = 8
     flags = 0
     s32 = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32, device=device, record_slots=rs, flags=flags)
+    if args.force_refresh:
+        s32.set_force_refresh(args.force_refresh)
     s64 = gfb.Solver(prob, dirs=dirs, precision=gfb.FP64, device=device, record_slots=rs, flags=flags)
     green = "recording" in prob and WORKLOADS[args.workload].get("tile") is not None
     out = {"workload": args.workload, "steps": n, "split_nodes": split_nodes(prob),
-           "inputs": "GPU generator" if args.gpu_prep else "host generator, numbering on the GPU"}
+           "inputs": "GPU generator" if args.gpu_prep else "host generator, numbering on the GPU",
+           "fp32_force_refresh": s32.info()["force_refresh"], "fp32_half_v": s32.info()["half_v"]}
     if args.workload == "halfspace_20x20x10":
         import oracle
 
@@ -959,6 +963,8 @@ def main():
     ap.add_argument("--accuracy", action="store_true",
                     help="measure the FP32 batched path's trace error over the workload's full run instead")
     ap.add_argument("--accuracy-steps", type=int, default=0, help="steps of --accuracy (default: the full run)")
+    ap.add_argument("--force-refresh", type=int, default=0,
+                    help="FP32 steps between full element-force evaluations (default: the solver's, 800)")
     ap.add_argument("--record-f64", dest="record_f32", action="store_false",
                     help="snapshots in double (default: float, the reference example's snapshot_precision)")
     args = ap.parse_args()

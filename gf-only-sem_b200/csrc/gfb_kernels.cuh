@@ -107,9 +107,10 @@ struct NodeArgs {
     // it adds the force of the step's increment (the node pass stores the
     // increment of the predicted displacement); nullptr: always in full
     const int* mnext;
-    // plain nodes keep the half-step velocity v + dt/2 a in v and no
-    // acceleration (see update_node_field)
+    // plain nodes keep the half-step velocity w = v + dt/2 a (in float, in
+    // w32 [node][3*n_field]) and no acceleration (see update_node_field)
     bool half_v;
+    float* w32;
 };
 
 // C-PML at global nodes (FP32 path).
@@ -407,12 +408,16 @@ __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const
         // displacement u_{n+1} + dt w_{n+1} (its increment dt w_{n+1}).  The
         // same values as the (u, v, a) form in exact arithmetic, without the
         // acceleration's read and write; v and a are recovered from w and
-        // the assembled force when they are needed (records, state).
+        // the assembled force when they are needed (records, state).  w is
+        // held in float (its rounding adds a random walk of ~1e-7 relative
+        // per step, far below the float rounding of the predicted
+        // displacement that bounds this path), u in double.
+        float* __restrict__ pw = A.w32 + i0;
         double uu[3], ww[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             uu[c] = pu[c];
-            ww[c] = pv[c];
+            ww[c] = (double)pw[c];
         }
         const Real im = __ldg(A.inv_mass + g);
         Real out[3];
@@ -421,9 +426,9 @@ __device__ __forceinline__ void update_node_field(const NodeArgs<Real>& A, const
             if (im != Real(0)) {  // m <= 0: the node stays as it is (a = 0, solver.cpp:58-61)
                 const double a_new = (double)(Real)(fv[c] * im);
                 uu[c] = dadd(uu[c], dmul(K.dt, ww[c]));
-                ww[c] = dadd(ww[c], dmul(K.dt, a_new));
+                ww[c] = (double)(float)dadd(ww[c], dmul(K.dt, a_new));
                 pu[c] = uu[c];
-                pv[c] = ww[c];
+                pw[c] = (float)ww[c];
             }
             out[c] = full ? (Real)dadd(uu[c], dmul(K.dt, ww[c])) : (Real)dmul(K.dt, ww[c]);
         }
@@ -1475,11 +1480,11 @@ __global__ void __launch_bounds__(ColShape<NG, NFLD, EPB_, XCH>::THREADS, ColSha
 }
 
 // Predictor only (start of a run or after a state overwrite).
-// Nodes g >= hv_begin hold the half-step velocity (v + dt/2 a) in v.
+// Nodes g >= hv_begin hold the half-step velocity (v + dt/2 a) in w32.
 template <typename Real>
 __global__ void predict_kernel(long long n_node, int F, const double* u, const double* v, const Real* a,
                                Real* ut, double dt, double half_dt2, const uint8_t* node_model,
-                               const ModelConst* mc, long long hv_begin) {
+                               const ModelConst* mc, long long hv_begin, const float* w32) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long total = n_node * F;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
@@ -1492,7 +1497,7 @@ __global__ void predict_kernel(long long n_node, int F, const double* u, const d
             h2 = K.half_dt2;
         }
         ut[padded_index(g, f, F)] =
-            g >= hv_begin ? (Real)(u[idx] + h * v[idx]) : (Real)(u[idx] + h * v[idx] + h2 * (double)a[idx]);
+            g >= hv_begin ? (Real)(u[idx] + h * (double)w32[idx]) : (Real)(u[idx] + h * v[idx] + h2 * (double)a[idx]);
         if (f % 3 == 2) ut[padded_index(g, f, F) + 1] = Real(0);
     }
 }
@@ -1509,9 +1514,10 @@ struct RecArgs {
     const Real* a;
     long long n_node;
     Out* out;               // [NFLD][n_rec][NN][15]
-    // nodes g >= hv_begin hold the half-step velocity: a = f/m from the
-    // step's assembled force, v = w - dt/2 a
+    // nodes g >= hv_begin hold the half-step velocity w (w32): a = f/m from
+    // the step's assembled force, v = w - dt/2 a
     long long hv_begin;
+    const float* w32;
     const Real* force;      // [node][NFLD][4]
     const Real* inv_mass;   // [node]
     const uint8_t* node_model;
@@ -1572,7 +1578,7 @@ __global__ void record_kernel(RecArgs<Real, Out> A) {
             for (int c = 0; c < 3; ++c) {
                 const double an = (double)(Real)(A.force[((size_t)g * NFLD + d) * 4 + c] * im);
                 o[6 + c] = (Out)A.u[(size_t)g * F + d * 3 + c];
-                o[9 + c] = (Out)(A.v[(size_t)g * F + d * 3 + c] - 0.5 * h * an);
+                o[9 + c] = (Out)((double)A.w32[(size_t)g * F + d * 3 + c] - 0.5 * h * an);
                 o[12 + c] = (Out)an;
             }
         } else {
@@ -1586,14 +1592,13 @@ __global__ void record_kernel(RecArgs<Real, Out> A) {
 }
 
 
-// Half-step velocity state <-> (v, a) at the nodes g >= hv_begin.
+// Half-step velocity state (w32) <-> (v, a) at the nodes g >= hv_begin.
 // to_full: v_out = w - dt/2 a, a_out = a with a = f/m from the assembled
 // force (a_from_force) or the stored a (state set since the last step);
-// otherwise (from_full): w = v + dt/2 a in place of v.  One thread per
-// (node, value).
+// otherwise (from_full): w = v + dt/2 a.  One thread per (node, value).
 template <typename Real>
 __global__ void half_v_kernel(long long n_node, int F, long long hv_begin, bool to_full, bool a_from_force,
-                              double* v, const Real* a, const Real* force, const Real* inv_mass,
+                              const double* v, float* w32, const Real* a, const Real* force, const Real* inv_mass,
                               const uint8_t* node_model, const ModelConst* mc, double dt, double* v_out,
                               Real* a_out) {
     const long long total = (n_node - hv_begin) * F;
@@ -1605,10 +1610,10 @@ __global__ void half_v_kernel(long long n_node, int F, long long hv_begin, bool 
         const double h = node_model ? mc[node_model[g]].dt : dt;
         if (to_full) {
             const double an = a_from_force ? (double)(Real)(force[padded_index(g, f, F)] * inv_mass[g]) : (double)a[i];
-            v_out[i] = v[i] - 0.5 * h * an;
+            v_out[i] = (double)w32[i] - 0.5 * h * an;
             a_out[i] = (Real)an;
         } else {
-            v[i] = v[i] + 0.5 * h * (double)a[i];
+            w32[i] = (float)(v[i] + 0.5 * h * (double)a[i]);
         }
     }
 }

@@ -36,8 +36,11 @@ thread_local std::string g_err;
 // to float, a perturbation the stiffness amplifies into the highest
 // (undamped) modes; by increments the rounded quantity is a step's change,
 // ~dt*omega smaller, and the periodic full evaluation keeps the float sum
-// of increments from drifting.
-constexpr int kRefreshSteps = 100;
+// of increments from drifting.  The acceleration error after the deformed
+// 128x128x64 run (6000 steps) was 1.0e-4 / 5.9e-5 / 5.2e-5 for periods of
+// 100 / 400 / 800 steps: the rounding of the increments grows like the
+// square root of the period, that of the full evaluations like their count.
+constexpr int kRefreshSteps = 800;
 
 gfb_status fail(gfb_status st, const char* fmt, ...) {
     char buf[1024];
@@ -311,6 +314,7 @@ struct gfb_solver {
     // one (state set since the last step)
     bool half_v = false;
     long long hv_begin = 0;
+    float* w32 = nullptr;              // [node][F] half-step velocity of the nodes >= hv_begin
     bool a_in_force = false;
     long long* d_stf_off = nullptr;
     void *d_mstf = nullptr, *d_stf_all = nullptr;
@@ -520,6 +524,7 @@ void node_args(const gfb_solver* s, gfb::NodeArgs<Real>& A, gfb::NodePml<Real>& 
     A.live_node_end = s->d_live_node_end;  // null with one model
     A.mnext = s->refresh > 1 ? s->d_mnext : nullptr;
     A.half_v = s->half_v;
+    A.w32 = s->w32;
     P = gfb::NodePml<Real>{};
     if (s->node_pml) {
         P.coef = static_cast<const Real*>(s->npml_coef);
@@ -721,6 +726,7 @@ gfb_status launch_record_o(gfb_solver* s, Out* out) {
     A.n_node = s->n_node;
     A.out = out;
     A.hv_begin = s->half_v ? s->hv_begin : s->n_node;
+    A.w32 = s->w32;
     A.force = static_cast<const Real*>(s->force);
     A.inv_mass = static_cast<const Real*>(s->inv_mass);
     A.node_model = s->d_node_model;
@@ -889,7 +895,7 @@ gfb_status launch_predict_t(gfb_solver* s) {
     const double h = 0.5 * s->dt * s->dt * (1.0 - 2.0 * 0.0);
     gfb::predict_kernel<Real><<<grid_for(n, 256), 256, 0, s->stream>>>(
         (long long)s->n_node, s->F, s->u, s->v, static_cast<const Real*>(s->a), static_cast<Real*>(s->ut), s->dt, h,
-        s->d_node_model, s->d_mc, s->half_v ? s->hv_begin : (long long)s->n_node);
+        s->d_node_model, s->d_mc, s->half_v ? s->hv_begin : (long long)s->n_node, s->w32);
     CU(cudaGetLastError());
     s->launches++;
     return GFB_OK;
@@ -901,7 +907,7 @@ gfb_status half_v_to_full(gfb_solver* s, double* v_out, float* a_out) {
     const long long total = (long long)(s->n_node - s->hv_begin) * s->F;
     if (total <= 0) return GFB_OK;
     gfb::half_v_kernel<float><<<grid_for(total, 256), 256, 0, s->stream>>>(
-        (long long)s->n_node, s->F, s->hv_begin, true, s->a_in_force, s->v, static_cast<const float*>(s->a),
+        (long long)s->n_node, s->F, s->hv_begin, true, s->a_in_force, s->v, s->w32, static_cast<const float*>(s->a),
         static_cast<const float*>(s->force), static_cast<const float*>(s->inv_mass), s->d_node_model, s->d_mc, s->dt,
         v_out, a_out);
     CU(cudaGetLastError());
@@ -914,7 +920,7 @@ gfb_status half_v_from_full(gfb_solver* s) {
     const long long total = (long long)(s->n_node - s->hv_begin) * s->F;
     if (total <= 0) return GFB_OK;
     gfb::half_v_kernel<float><<<grid_for(total, 256), 256, 0, s->stream>>>(
-        (long long)s->n_node, s->F, s->hv_begin, false, false, s->v, static_cast<const float*>(s->a), nullptr,
+        (long long)s->n_node, s->F, s->hv_begin, false, false, s->v, s->w32, static_cast<const float*>(s->a), nullptr,
         nullptr, s->d_node_model, s->d_mc, s->dt, nullptr, nullptr);
     CU(cudaGetLastError());
     s->launches++;
@@ -1969,6 +1975,10 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     s->half_v = s->prec == GFB_FP32 && (!s->has_cpml || s->node_pml) && !s->fuse && !s->has_damping &&
                 !(c->flags & GFB_FLAG_DIRECT_FORCE);
     s->hv_begin = s->half_v ? (s->node_pml ? s->n_pml_node : 0) : s->n_node;
+    if (s->half_v) {  // the state starts at rest: w = 0
+        if ((st = s->alloc(&s->w32, (size_t)s->n_node * s->F))) return st;
+        CU(cudaMemsetAsync(s->w32, 0, (size_t)s->n_node * s->F * sizeof(float), s->stream));
+    }
     if ((c->flags & GFB_FLAG_AUTOTUNE) && (st = autotune(s.get()))) return st;
     CU(cudaDeviceSynchronize());
     clk.mark("autotune");
@@ -2187,6 +2197,22 @@ gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
     return GFB_OK;
 }
 
+gfb_status gfb_set_force_refresh(gfb_solver* s, int32_t steps) {
+    if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
+    if (steps < 1) return fail(GFB_ERR_INVALID, "force refresh period must be >= 1");
+    if (s->refresh <= 1 && steps > 1)
+        return fail(GFB_ERR_UNSUPPORTED, "this solver evaluates the element force in full every step");
+    gfb_status st;
+    CU(cudaStreamSynchronize(s->stream));
+    if (s->refresh > 1 && (st = launch_predict(s))) return st;  // the next step evaluates in full
+    s->refresh = steps;
+    if (s->gexec) {
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
+    return GFB_OK;
+}
+
 gfb_status gfb_select_element_kernel(gfb_solver* s, int32_t variant) {
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (!col_kernel_eligible(s)) return fail(GFB_ERR_UNSUPPORTED, "this solver has one element kernel");
@@ -2355,6 +2381,7 @@ std::vector<std::pair<void*, size_t>> checkpoint_arrays(gfb_solver* s) {
         a.push_back({s->npml_prev, (size_t)s->n_pml_node * s->F * es});
     }
     a.push_back({s->d_mstep, (size_t)s->n_model * 4});
+    if (s->half_v) a.push_back({s->w32, (size_t)s->n_node * s->F * 4});
     if (s->refresh > 1) {
         // the stored force is state when it is updated by increments
         a.push_back({s->force, (size_t)s->n_node * s->nfld * 4 * es});

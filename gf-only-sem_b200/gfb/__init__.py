@@ -154,6 +154,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                        _ip, _ip, C.POINTER(C.c_void_p)]
     lib.gfb_get_info.argtypes = [C.c_void_p, C.POINTER(Info)]
     lib.gfb_select_element_kernel.argtypes = [C.c_void_p, C.c_int32]
+    lib.gfb_set_force_refresh.argtypes = [C.c_void_p, C.c_int32]
     lib.gfb_current_step.argtypes = [C.c_void_p, _ip]
     lib.gfb_get_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
     lib.gfb_set_state.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp, _dp]
@@ -170,7 +171,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "gfb_element_residual", "gfb_advance_profiled", "gfb_get_info", "gfb_advance_timed",
         "gfb_create_batch", "gfb_checkpoint_size", "gfb_checkpoint_save", "gfb_checkpoint_load",
         "gfb_rec_nodes", "gfb_read_green", "gfb_read_record_f32", "gfb_create_sources",
-        "gfb_select_element_kernel",
+        "gfb_select_element_kernel", "gfb_set_force_refresh",
     ):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -352,6 +353,10 @@ class Solver:
         """Use element-kernel variant `variant` from the next step on (-1: the
         thread-per-point kernel; 0..n_elem_variants-1: the line kernel's)."""
         _check(self.lib.gfb_select_element_kernel(self.h, int(variant)))
+
+    def set_force_refresh(self, steps: int):
+        """FP32 path: steps between full evaluations of the element force."""
+        _check(self.lib.gfb_set_force_refresh(self.h, int(steps)))
 
     def synchronize(self):
         _check(self.lib.gfb_synchronize(self.h))

@@ -114,8 +114,8 @@ typedef struct gfb_config {
 /* FP32 path: evaluate the element force from the full predicted
  * displacement at every step.  By default most steps add the force of the
  * predicted displacement's increment over the previous step to the stored
- * force, with a full evaluation every 100 steps (and after the state is
- * overwritten): the float rounding of the full predicted displacement,
+ * force, with a full evaluation every 800 steps (and after the state is
+ * overwritten; gfb_set_force_refresh changes the period): the float rounding of the full predicted displacement,
  * amplified by the stiffness into the highest modes, is what bounds the
  * FP32 path's accuracy (recorded acceleration ~1.5e-4 relative L2 after
  * 2000 steps in full, ~3e-5 by increments).  Applies only where the C-PML
@@ -264,6 +264,14 @@ typedef struct gfb_info {
 } gfb_info;
 
 gfb_status gfb_get_info(const gfb_solver* solver, gfb_info* info);
+
+/* FP32 path: steps between full evaluations of the element force (the steps
+ * between add the force of the predicted displacement's increment; 800 by
+ * default, 1 = in full every step).  The next step evaluates in full.
+ * GFB_ERR_UNSUPPORTED for a period > 1 on a solver that evaluates in full
+ * every step (FP64, per-cell C-PML, fused node update, GFB_FLAG_DIRECT_FORCE,
+ * a learned layer attached). */
+gfb_status gfb_set_force_refresh(gfb_solver* solver, int32_t steps);
 
 /* Use element-kernel variant `variant` (as in gfb_info.elem_variant) from
  * the next step on, in place of the autotuner's or the default choice; the

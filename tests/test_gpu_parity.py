@@ -307,7 +307,7 @@ def test_fp32_line_kernel_variants_agree(dirs):
         for k in ("u", "strain"):
             assert rel_l2(runs[3][f][k], runs[0][f][k]) < 1e-5
     # switching kernels between steps (the next step evaluates in full, off
-    # the 100-step schedule): still within 1e-4 of the oracle
+    # the refresh schedule): still within 1e-4 of the oracle
     s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
     s.advance(n // 3)
     s.select_element_kernel(3)
@@ -466,7 +466,7 @@ def test_source_sets_are_checked():
 def test_fp32_force_by_increments_against_full_evaluation():
     """FP32 path: the element force of most steps is the stored force plus
     the force of the predicted displacement's increment (full evaluation
-    every 100 steps, and after a state overwrite); evaluating it in full
+    every 800 steps, and after a state overwrite); evaluating it in full
     every step (GFB_FLAG_DIRECT_FORCE) gives the same traces to FP32 rounding,
     both within 1e-4 of the FP64 oracle, and a resume through set_state
     continues correctly."""
@@ -493,3 +493,49 @@ def test_fp32_force_by_increments_against_full_evaluation():
     inc2.advance(260)
     for f in range(3):
         assert rel_l2(res.state(f)[0], inc2.state(f)[0]) < FP32_TOL
+
+
+def test_force_refresh_period_is_settable_and_checked():
+    """gfb_set_force_refresh: every period gives traces within 1e-4 of the
+    FP64 oracle (1: in full every step, as GFB_FLAG_DIRECT_FORCE, which also
+    keeps (v, a) at every node: the same traces to rounding); a period of 1
+    after increments, and a change mid-run, evaluate the next step in full;
+    a solver that evaluates in full every step rejects a longer period."""
+    prob = layered_problem(nsteps=240)
+    n = prob["nsteps"]
+    runs = {}
+    for period in (1, 7, 50, 1000):
+        s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32)
+        s.set_force_refresh(period)
+        assert s.info()["force_refresh"] == period
+        s.advance(n)
+        runs[period] = s.drain()
+        s.close()
+    full = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, flags=gfb.FLAG_DIRECT_FORCE)
+    full.advance(n)
+    direct = full.drain()
+    full.close()
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        for period, snaps in runs.items():
+            compare_runs(snaps[d], ref, FP32_TOL, f"refresh {period} field {d}")
+        for k in ("strain", "u"):
+            assert rel_l2(runs[1][d][k], direct[d][k]) < 1e-5
+    s = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32)
+    s.advance(n // 3)
+    s.set_force_refresh(3)
+    s.advance(n // 3)
+    s.set_force_refresh(1)
+    s.advance(n - 2 * (n // 3))
+    mixed = s.drain()
+    s.close()
+    for d in range(3):
+        ref, _ = oracle_snaps(prob, d, n)
+        compare_runs(mixed[d], ref, FP32_TOL, f"changed refresh field {d}")
+    with pytest.raises(gfb.GfbError, match=">= 1"):
+        gfb.Solver(prob, dirs=[0], precision=gfb.FP32).set_force_refresh(0)
+    s64 = gfb.Solver(prob, dirs=[0], precision=gfb.FP64)
+    s64.set_force_refresh(1)  # what it does anyway
+    with pytest.raises(gfb.GfbError, match="in full every step"):
+        s64.set_force_refresh(100)
+    s64.close()
