@@ -464,7 +464,7 @@ def node_bytes_per_step(prob, info, n_field, prec):
 
 
 def committed_traffic():
-    path = os.path.join(REPO, "profiles", "elem_col_traffic_deformed_32x32x16.json")
+    path = os.path.join(REPO, "profiles", "elem_col_traffic_deformed_64x64x32.json")
     try:
         with open(path) as f:
             return json.load(f)
@@ -797,10 +797,13 @@ def run_gfb(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == gfb.FP32 else "f64",
         "data": "synthetic",
         "config": {"workload": args.workload, "n_cell": prob["n_cell"], "ngll": 5, "n_node": prob["n_node"],
-                   "fields": len(dirs), "precision": args.precision, "state": "f64 u,v",
+                   "fields": len(dirs), "precision": args.precision,
+                   "state": ("f64 u, f32 half-step velocity at the plain nodes, f64 u,v + f32 a at the C-PML nodes"
+                             if info["half_v"] else "f64 u,v"),
                    "l2": "inputs larger than L2 (geometry alone > 700 MB)", "parallelism": f"replicas{world}",
                    "n_colour": info["n_colour"], "n_pml_cell": info["n_pml_cell"],
-                   "elem_blocks": info["elem_blocks"],
+                   "elem_blocks": info["elem_blocks"], "elem_variant": info["elem_variant"],
+                   "force_refresh": info["force_refresh"],
                    "inputs": (f"GPU generator (gfb.prep, crack-free coordinates), {t_gen:.1f} s" if args.gpu_prep
                               else f"host generator (the reference preprocessor's arithmetic; numbering of its "
                                    f"points on the GPU, the same ids as the host lexsort), {t_gen:.1f} s"),

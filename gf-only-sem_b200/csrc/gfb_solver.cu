@@ -264,7 +264,7 @@ struct gfb_solver {
     uint32_t* ibool_padded = nullptr;  // [cell][NNP] for the pipelined kernel
     int pipe_blocks = 0;               // persistent grid of the element kernel
     int col_blocks = 0;                // persistent grid of the line kernel (FP32)
-    int col_variant = 0;               // cells per group: 0 default, 1 fewer, 2 more; 3 default, line owners
+    int col_variant = 0;               // line kernel: 0 default (line owners where built), 1 fewer cells, 2 more, 3 default cells, exchange by every thread
     int n_col_variants = 1;
     int col_epb = 0;                   // cells per group of the variant in use
     bool point_kernel = false;         // thread-per-point element kernel on the FP32 path
@@ -628,9 +628,12 @@ gfb_status launch_col_e(gfb_solver* s, int c) {
     return GFB_OK;
 }
 
-// Candidates of the line kernel: the default cells per group, and at
-// ngll 5 one fewer ("LO") and one more ("HI") step, and the default with
-// the eta/zeta contractions done by line owners (ColShape's XCH).
+// Candidates of the line kernel.  At ngll 5 with up to three wavefields:
+// 0 the default cells per group with the eta/zeta contractions done by line
+// owners (ColShape's XCH; the fastest measured), and with the exchange done
+// by every thread 1 one fewer cell per group ("LO"), 2 one more ("HI"),
+// 3 the default count.  Elsewhere: 0 the default count, exchange by every
+// thread.
 constexpr int col_epb_lo(int nfld) { return nfld == 3 ? 1 : (nfld == 2 ? 2 : 4); }
 constexpr int col_epb_hi(int nfld) { return nfld == 3 ? 3 : (nfld == 2 ? 4 : 8); }
 template <int NG, int NFLD>
@@ -645,9 +648,9 @@ template <int NG, int NFLD>
 gfb_status launch_col_t(gfb_solver* s, int c) {
     using E = ColEpb<NG, NFLD>;
     if constexpr (E::N > 1) {
+        if (s->col_variant == 0) return launch_col_e<NG, NFLD, E::D, true>(s, c);
         if (s->col_variant == 1) return launch_col_e<NG, NFLD, col_epb_lo(NFLD)>(s, c);
         if (s->col_variant == 2) return launch_col_e<NG, NFLD, col_epb_hi(NFLD)>(s, c);
-        if (s->col_variant == 3) return launch_col_e<NG, NFLD, E::D, true>(s, c);
     }
     return launch_col_e<NG, NFLD, E::D>(s, c);
 }
@@ -681,7 +684,7 @@ gfb_status col_grid_t(gfb_solver* s) {
             s->col_epb = col_epb_hi(NFLD);
             return col_grid<NG, NFLD, col_epb_hi(NFLD)>(s, &s->col_blocks);
         }
-        if (s->col_variant == 3) {
+        if (s->col_variant == 0) {
             s->col_epb = E::D;
             return col_grid<NG, NFLD, E::D, true>(s, &s->col_blocks);
         }

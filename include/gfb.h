@@ -258,7 +258,10 @@ typedef struct gfb_info {
     int32_t force_refresh;   /* steps between full element-force evaluations (1: every step) */
     int32_t half_v;          /* 1: plain nodes keep the half-step velocity, no acceleration */
     int32_t elem_variant;    /* FP32 element kernel in use: -1 thread-per-point; line kernel
-                                with 0 the default cells per group, 1 fewer, 2 more           */
+                                0 the default (at ngll 5 with <= 3 wavefields: eta/zeta
+                                contractions by line owners); there also 1 one fewer cell
+                                per group, 2 one more, 3 the default count, the exchange
+                                done by every thread                                         */
     int32_t n_elem_variants; /* line-kernel variants built for this ngll / field count
                                 (0: the solver has one element kernel)                        */
 } gfb_info;

@@ -278,11 +278,12 @@ def test_fp32_line_and_point_kernels_agree():
 
 @pytest.mark.parametrize("dirs", [[2], [0, 1], [0, 1, 2]])
 def test_fp32_line_kernel_variants_agree(dirs):
-    """Every variant of the line kernel at order 4: cells per group default,
-    fewer, more (the same sums in the same order per xi-line, so the traces
-    are bit-identical to the default variant's) and the line-owner exchange
-    (the eta and zeta sums added in another order: within 1e-5); all within
-    1e-4 of the oracle; and kernels switched between steps."""
+    """Every variant of the line kernel at order 4: the default (line-owner
+    exchange) and, with the exchange done by every thread, cells per group
+    fewer, more and default (the same sums in the same order per xi-line:
+    bit-identical to each other; the line owners add the eta and zeta sums
+    in another order: within 1e-5); all within 1e-4 of the oracle; and
+    kernels switched between steps."""
     n = 120
     prob = layered_problem(nsteps=n)
     runs = {}
@@ -299,13 +300,13 @@ def test_fp32_line_kernel_variants_agree(dirs):
         s.close()
     for f, d in enumerate(dirs):
         ref, _ = oracle_snaps(prob, d, n)
-        compare_runs(runs[0][f], ref, FP32_TOL, f"line kernel field {d}")
-        compare_runs(runs[3][f], ref, FP32_TOL, f"line-owner exchange field {d}")
+        compare_runs(runs[0][f], ref, FP32_TOL, f"line-owner exchange field {d}")
+        compare_runs(runs[3][f], ref, FP32_TOL, f"exchange by every thread field {d}")
         for v in (1, 2):
             for k in ("strain", "u", "v", "a"):
-                np.testing.assert_array_equal(runs[v][f][k], runs[0][f][k], err_msg=f"variant {v} {k}")
+                np.testing.assert_array_equal(runs[v][f][k], runs[3][f][k], err_msg=f"variant {v} {k}")
         for k in ("u", "strain"):
-            assert rel_l2(runs[3][f][k], runs[0][f][k]) < 1e-5
+            assert rel_l2(runs[0][f][k], runs[3][f][k]) < 1e-5
     # switching kernels between steps (the next step evaluates in full, off
     # the refresh schedule): still within 1e-4 of the oracle
     s = gfb.Solver(prob, dirs=dirs, precision=gfb.FP32)
