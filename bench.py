@@ -699,7 +699,12 @@ def run_gfb(args):
     prec = gfb.FP32 if args.precision == "fp32" else gfb.FP64
     dirs = [0, 1, 2][: args.fields]
     t_gen = time.perf_counter()
-    prob = build_workload(args.workload, prep="gpu" if args.gpu_prep else "reference", device=device)
+    # the ranks of one node generate their inputs at the same time: each
+    # takes its share of the host cores
+    from gfb.workloads import host_threads
+    threads = max(1, host_threads() // max(1, int(os.environ.get("LOCAL_WORLD_SIZE", "1"))))
+    prob = build_workload(args.workload, prep="gpu" if args.gpu_prep else "reference", device=device,
+                          threads=threads)
     t_gen = time.perf_counter() - t_gen
     flags = (gfb.FLAG_RECORD_F32 if args.record_f32 else 0) | (gfb.FLAG_POINT_KERNEL if args.point_kernel else 0)
     s = gfb.Solver(prob, dirs=dirs, precision=prec, device=device, record_slots=8, flags=flags)
