@@ -217,8 +217,15 @@ def run_layer(args):
     all_planes = tuple(range(5))
     for name, wts, planes in (("untrained", zero, None), ("trained", params, None),
                               ("untrained, 5 planes", zero, all_planes)):
+        init = None
+        if planes:
+            # start from the truncation surface's fit with the inner planes
+            # undamped (unit damping on every plane reflects strongly)
+            surface = sorted(set(int(k) for k in gl.Layer(cases[0].thin).net))
+            init = np.full_like(fits["untrained"]["gains"], np.exp(-gl.LOG_GAIN_BOUND))
+            init[surface] = fits["untrained"]["gains"][surface]
         g, e, hist = gl.fit_gains(cases, wts, scales, max_evals=w["loop_evals"] * (3 if planes else 1),
-                                  device=args.device, planes=planes)
+                                  device=args.device, planes=planes, init=init)
         fits[name] = dict(gains=g, train_error=e, start_error=hist[0][1], evals=hist[-1][0], planes=planes,
                           weights=wts)
     for c in cases:

@@ -502,18 +502,21 @@ LOG_GAIN_BOUND = 6.0  # gains within e^-6 .. e^6 (the kernel caps the damping at
 
 
 def fit_gains(cases, params: np.ndarray, scales: np.ndarray, nets=None, step: float = 1.0,
-              min_step: float = 0.125, max_evals: int = 120, device: int = 0, planes=None):
+              min_step: float = 0.125, max_evals: int = 120, device: int = 0, planes=None,
+              init: Optional[np.ndarray] = None):
     """Closed-loop stage of training: the damping gains [n_net][3] (one per
     network and face axis) that minimise the reflection error of whole runs
     of the training cases with the given networks, by coordinate search on
     log-gains (steps +-step, halved when a sweep brings no improvement,
     down to min_step).  ``nets``: the networks whose gains are fitted
     (default: those with nodes in the first case's layer; ``planes`` as in
-    layer_nodes).  Returns (gains, error, history of (evaluations, error))."""
+    layer_nodes); ``init``: starting gains [n_net][3] (default 1).  Returns
+    (gains, error, history of (evaluations, error))."""
     n_net = params.shape[0]
     if nets is None:
         nets = sorted(set(int(k) for k in Layer(cases[0].thin, planes).net))
-    lg = np.zeros((n_net, 3))
+    lg = np.zeros((n_net, 3)) if init is None else np.clip(np.log(np.maximum(np.asarray(init, dtype=np.float64),
+                                                                            1e-30)), -LOG_GAIN_BOUND, LOG_GAIN_BOUND)
     best = loop_error(cases, params, scales, np.exp(lg), 1.0, device, planes)
     evals, hist = 1, [(1, best)]
     while step >= min_step and evals < max_evals:
