@@ -10,6 +10,9 @@ example configures it.
 * FP32 batched x/y/z path: <= 1e-4 against the same CPU run for x, and
   against the FP64 GPU path (validated above) for x, y and z.
 
+And the layered 64 x 64 x 32 workload over its 4000 steps: FP32 batched
+x/y/z against the FP64 path, <= 1e-4.
+
 The errors are accumulated snapshot by snapshot (gfb.accuracy.TraceError):
 ||gpu - ref|| / ||ref|| over all snapshots, cells, points and components.
 """
@@ -74,3 +77,25 @@ def test_halfspace_2000_steps_fp64_and_fp32_against_the_cpu_reference():
     for k, v in final.items():
         assert v <= FP64_TOL, (k, v)
     assert e32_64.worst() <= FP32_TOL, e32_64.summary()
+
+
+def test_layered_64x64x32_4000_steps_fp32_within_1e4_of_fp64():
+    """The layered 64 x 64 x 32 workload (131,072 cells, 4-cell C-PML, 4000
+    steps, 400 snapshots of the surface cells) with the
+    host generator's inputs: the FP32 batched x/y/z path against the FP64
+    path (validated against the reference's CPU functions above) over the
+    whole run, every snapshot, every quantity <= 1e-4."""
+    from gfb.accuracy import compare_solvers
+
+    prob = build_workload("layered_64x64x32", prep="reference", device=0)
+    n = prob["nsteps"]
+    assert n == 4000
+    s32 = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP32, record_slots=8)
+    s64 = gfb.Solver(prob, dirs=[0, 1, 2], precision=gfb.FP64, record_slots=8)
+    assert s32.info()["force_refresh"] > 1 and s32.info()["half_v"] == 1
+    err = compare_solvers(s32, s64, n, chunk=8 * int(prob["snapshot_stride"]))
+    s32.close()
+    s64.close()
+    print(f"fp32 vs fp64, layered 64x64x32, {n} steps: {err.summary()}")
+    assert err.snapshots == 400
+    assert err.worst() <= FP32_TOL, err.summary()
