@@ -306,6 +306,7 @@ struct gfb_solver {
     // (FP32 path; 1 = in full every step): per model this step's kind, the
     // next step's kind and a one-shot request for a full step
     int refresh = 1;
+    bool by_increments_ok = false;     // the force may be updated by increments (FP32, node-form or no C-PML, ...)
     int *d_mdirect = nullptr, *d_mnext = nullptr, *d_force_direct = nullptr;
     int* d_kernel_err = nullptr;       // set by a kernel whose bounded wait gave up
     // plain nodes (device nodes >= hv_begin) keep the half-step velocity
@@ -1967,10 +1968,9 @@ gfb_status create_impl(const gfb_mesh* m, const gfb_config* c, const gfb_source*
     // displacement's increment (see step_begin_kernel), where the C-PML
     // term is added at the nodes (node form or none) and no node is
     // finalised inside the element kernel
-    s->refresh = (s->prec == GFB_FP32 && (!s->has_cpml || s->node_pml) && !s->fuse &&
-                  !(c->flags & GFB_FLAG_DIRECT_FORCE))
-                     ? kRefreshSteps
-                     : 1;
+    s->by_increments_ok = s->prec == GFB_FP32 && (!s->has_cpml || s->node_pml) && !s->fuse &&
+                          !(c->flags & GFB_FLAG_DIRECT_FORCE);
+    s->refresh = s->by_increments_ok ? kRefreshSteps : 1;
     // plain nodes in the half-step velocity form where nothing reads their
     // (v, a) inside the step: the FP32 path with node-form or no C-PML, no
     // legacy damping (it acts on v_n, solver.cpp:564-574), no node update in
@@ -2203,12 +2203,17 @@ gfb_status gfb_get_info(const gfb_solver* s, gfb_info* info) {
 gfb_status gfb_set_force_refresh(gfb_solver* s, int32_t steps) {
     if (!s) return fail(GFB_ERR_INVALID, "solver is NULL");
     if (steps < 1) return fail(GFB_ERR_INVALID, "force refresh period must be >= 1");
-    if (s->refresh <= 1 && steps > 1)
+    if (steps > 1 && !s->by_increments_ok)
         return fail(GFB_ERR_UNSUPPORTED, "this solver evaluates the element force in full every step");
     gfb_status st;
     CU(cudaStreamSynchronize(s->stream));
-    if (s->refresh > 1 && (st = launch_predict(s))) return st;  // the next step evaluates in full
+    // between full evaluations the node pass leaves the predicted
+    // displacement's increment in place of it: rewrite it in full
+    if (s->refresh > 1 && (st = launch_predict(s))) return st;
     s->refresh = steps;
+    // the next step evaluates the force in full (from a period of 1 the
+    // stored force is this step's, but the next step must not add to it)
+    if (steps > 1) CU(cudaMemsetAsync(s->d_force_direct, 1, (size_t)s->n_model * sizeof(int), s->stream));
     if (s->gexec) {
         cudaGraphExecDestroy(s->gexec);
         s->gexec = nullptr;
@@ -2711,6 +2716,7 @@ gfb_status solver_set_layer(gfb_solver* s, Layer* layer) {
         gfb_status st = leave_half_v(s);
         if (st) return st;
     }
+    if (layer) s->by_increments_ok = false;
     if (layer && s->refresh > 1) {
         // the layer adds its correction to the assembled force each step,
         // which must not accumulate: the force is evaluated in full from now

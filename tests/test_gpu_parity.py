@@ -527,7 +527,10 @@ def test_force_refresh_period_is_settable_and_checked():
     s.set_force_refresh(3)
     s.advance(n // 3)
     s.set_force_refresh(1)
-    s.advance(n - 2 * (n // 3))
+    s.advance(n // 6)
+    s.set_force_refresh(40)  # back to increments
+    assert s.info()["force_refresh"] == 40
+    s.advance(n - 2 * (n // 3) - n // 6)
     mixed = s.drain()
     s.close()
     for d in range(3):
