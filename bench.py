@@ -228,6 +228,13 @@ def run_layer(args):
                                   device=args.device, planes=planes, init=init)
         fits[name] = dict(gains=g, train_error=e, start_error=hist[0][1], evals=hist[-1][0], planes=planes,
                           weights=wts)
+    # then the replay-trained networks' output rows, with their gains: how
+    # much of each axis's damping follows the network's reading of the history
+    ft = fits["trained"]
+    wts, alpha, e, hist = gl.fit_output_layer(cases, params, scales, ft["gains"], max_evals=w["loop_evals"],
+                                              device=args.device)
+    fits["trained, output rows"] = dict(gains=ft["gains"], train_error=e, start_error=hist[0][1],
+                                        evals=hist[-1][0], planes=None, weights=wts, alpha=alpha)
     for c in cases:
         c.close()
     del cases
@@ -301,6 +308,9 @@ def run_layer(args):
                               f"cells, {w['loop_steps']} steps",
                         **{name: {"gains": {f"net {k}": [float(x) for x in f["gains"][k]]
                                             for k in sorted(set(int(q) for q in gl.Layer(thin, f["planes"]).net))},
+                                  **({"output_row_factors": {f"net {k}": [float(x) for x in f["alpha"][k]]
+                                                             for k in sorted(set(int(q) for q in gl.Layer(thin).net))}}
+                                     if "alpha" in f else {}),
                                   "train_error_start": f["start_error"], "train_error_fitted": f["train_error"],
                                   "evaluations": f["evals"]} for name, f in fits.items()}},
         "selection": {"on": f"2 held-out models {w['val_ni']}x{w['val_ni']}x{w['val_nk']} cells, "

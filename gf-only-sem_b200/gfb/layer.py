@@ -539,3 +539,56 @@ def fit_gains(cases, params: np.ndarray, scales: np.ndarray, nets=None, step: fl
         if not improved:
             step *= 0.5
     return np.exp(lg).astype(np.float32), best, hist
+
+
+W3_OFFSET = N_IN * N_HID + N_HID * N_HID  # W3 [3][64] in the FP32 parameters of a network
+
+
+def scale_output_rows(params: np.ndarray, alpha: np.ndarray) -> np.ndarray:
+    """Parameters with row j of network k's output layer W3 times
+    alpha[k][j] (alpha 0: the constant damping softplus(0) on that axis;
+    1: the network as given)."""
+    p = np.array(params, dtype=np.float32, copy=True)
+    w3 = p[:, W3_OFFSET:W3_OFFSET + N_OUT * N_HID].reshape(p.shape[0], N_OUT, N_HID)
+    w3 *= np.asarray(alpha, dtype=np.float32)[:, :, None]
+    return p
+
+
+def fit_output_layer(cases, params: np.ndarray, scales: np.ndarray, gains: Optional[np.ndarray] = None,
+                     nets=None, step: float = 0.5, min_step: float = 0.0625, max_alpha: float = 4.0,
+                     max_evals: int = 60, device: int = 0, planes=None):
+    """Closed-loop stage for the networks' output layer: a factor alpha per
+    network and face axis on the rows of W3 (how much of the damping
+    follows the network's reading of the node's history rather than the
+    constant softplus(0)), fitted to the reflection error of whole runs of
+    the training cases by coordinate search (steps +-step on alpha in
+    [0, max_alpha], halved when a sweep brings no improvement, down to
+    min_step), starting from the network as given (alpha = 1) with the
+    given damping gains.  Returns (params with the fitted rows, alpha,
+    error, history of (evaluations, error))."""
+    n_net = params.shape[0]
+    if nets is None:
+        nets = sorted(set(int(k) for k in Layer(cases[0].thin, planes).net))
+    alpha = np.ones((n_net, N_OUT))
+    best = loop_error(cases, scale_output_rows(params, alpha), scales, gains, 1.0, device, planes)
+    evals, hist = 1, [(1, best)]
+    while step >= min_step and evals < max_evals:
+        improved = False
+        for k in nets:
+            for j in range(N_OUT):
+                for sgn in (1.0, -1.0):
+                    if evals >= max_evals:
+                        break
+                    trial = alpha.copy()
+                    trial[k, j] = np.clip(trial[k, j] + sgn * step, 0.0, max_alpha)
+                    if trial[k, j] == alpha[k, j]:
+                        continue
+                    e = loop_error(cases, scale_output_rows(params, trial), scales, gains, 1.0, device, planes)
+                    evals += 1
+                    if e < best:
+                        best, alpha, improved = e, trial, True
+                        hist.append((evals, best))
+                        break
+        if not improved:
+            step *= 0.5
+    return scale_output_rows(params, alpha), alpha.astype(np.float32), best, hist

@@ -38,3 +38,27 @@ def test_fit_gains_respects_the_bound_and_the_evaluation_budget(monkeypatch):
     np.testing.assert_allclose(np.log(gains[4]), gl.LOG_GAIN_BOUND, atol=1e-6)
     gains, err, hist = gl.fit_gains([None], params, np.ones(4), nets=[4], max_evals=5)
     assert hist[-1][0] <= 5
+
+
+def test_fit_output_layer_finds_the_row_factors_of_a_synthetic_objective(monkeypatch):
+    rng = np.random.default_rng(3)
+    params = rng.normal(0.0, 0.1, size=(10, gl.N_PARAMS)).astype(np.float32)
+    sl = slice(gl.W3_OFFSET, gl.W3_OFFSET + gl.N_OUT * gl.N_HID)
+    want = np.ones((10, 3))
+    want[4] = [0.0, 2.0, 1.5]
+    want[9] = [0.5, 0.75, 3.0]
+    target = gl.scale_output_rows(params, want)
+
+    def fake_loop_error(cases, p, scales, gains, scale_mult=1.0, device=0, planes=None):
+        return float(np.sum((p[:, sl] - target[:, sl]) ** 2))
+
+    monkeypatch.setattr(gl, "loop_error", fake_loop_error)
+    fitted, alpha, err, hist = gl.fit_output_layer([None], params, np.ones(4), nets=[4, 9], max_evals=300)
+    np.testing.assert_allclose(alpha[[4, 9]], want[[4, 9]], atol=0.07)
+    np.testing.assert_array_equal(alpha[[0, 1, 2, 3, 5, 6, 7, 8]], 1.0)
+    assert err < 1e-2 * hist[0][1]
+    assert all(e2 < e1 for (_, e1), (_, e2) in zip(hist, hist[1:]))
+    keep = np.ones(gl.N_PARAMS, dtype=bool)
+    keep[sl] = False
+    np.testing.assert_array_equal(fitted[:, keep], params[:, keep])  # hidden layers untouched
+    np.testing.assert_allclose(gl.scale_output_rows(params, np.zeros((10, 3)))[:, sl], 0.0)
