@@ -248,6 +248,11 @@ def test_trained_layer_reduces_reflection_against_thick_cpml():
     gains, e_fit, hist = gl.fit_gains(cases, zero, scales, max_evals=30)
     assert e_fit < hist[0][1]  # the closed loop lowered the training error
     assert gains.shape == (n_net, 3) and np.all(gains > 0)
+    # the output-row factors of the replay-trained networks: never worse
+    # than where they start (the networks as trained, with these gains)
+    fitted, alpha, e_rows, hist_rows = gl.fit_output_layer(cases, params, scales, gains, max_evals=8)
+    assert e_rows <= hist_rows[0][1] and np.all((alpha >= 0) & (alpha <= 4))
+    assert np.isfinite(e_rows) and fitted.shape == params.shape
 
     test = gl.loop_case(pair(99, 500), dirs=(0, 1, 2))
     e_plain = gl.loop_error([test])
