@@ -822,7 +822,10 @@ def run_gfb(args):
                    "fields": len(dirs), "precision": args.precision,
                    "state": ("f64 u, f32 half-step velocity at the plain nodes, f64 u,v + f32 a at the C-PML nodes"
                              if info["half_v"] else "f64 u,v"),
-                   "l2": "inputs larger than L2 (geometry alone > 700 MB)", "parallelism": f"replicas{world}",
+                   "l2": (f"inputs larger than L2 (geometry alone {prob['n_cell'] * 6000 / 1e6:.0f} MB)"
+                          if prob["n_cell"] * 6000 > 126e6 else
+                          f"inputs partly L2-resident (geometry {prob['n_cell'] * 6000 / 1e6:.0f} MB, L2 126 MB)"),
+                   "parallelism": f"replicas{world}",
                    "n_colour": info["n_colour"], "n_pml_cell": info["n_pml_cell"],
                    "elem_blocks": info["elem_blocks"], "elem_variant": info["elem_variant"],
                    "force_refresh": info["force_refresh"],
